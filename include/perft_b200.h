@@ -1,0 +1,147 @@
+/*
+ * perft_b200 — C ABI of the B200 perft engine.
+ *
+ * Drop-in boundary for the perft path of ankan-ban/perft_gpu.  The reference
+ * exposes no library: its entry points are internal C++ functions behind the
+ * `perft_gpu <fen> <depth>` command line (perft.cu:14-164).  Each function
+ * below replaces one of them; the citation names the reference routine.
+ *
+ * Positions use the reference's 48-byte HexaBitBoardPosition layout
+ * (chess.h:208-230), so a caller holding reference positions passes them
+ * unchanged.  Counts are exact uint64 leaf counts.  Every entry point returns
+ * a status code (PERFT_OK or a negative PERFT_ERR_*) instead of the
+ * reference's printf/exit(0) and ALLSET sentinel (perft_bb.h:1360,1499).
+ *
+ * The entry points are thread-safe: calls on one process-wide engine are
+ * serialised by an internal lock.  All perft computation runs on the GPU;
+ * there is no CPU fallback — without a usable CUDA device, perft_init fails
+ * with PERFT_ERR_NO_DEVICE.
+ */
+#ifndef PERFT_B200_H
+#define PERFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define PERFT_OK                   0
+#define PERFT_ERR_INVALID_ARG     -1
+#define PERFT_ERR_NOT_INITIALIZED -2
+#define PERFT_ERR_CUDA            -3
+#define PERFT_ERR_OUT_OF_MEMORY   -4  /* replaces the reference's ALLSET sentinel */
+#define PERFT_ERR_INTERNAL        -5  /* a device-side consistency check failed */
+#define PERFT_ERR_BAD_FEN         -6
+#define PERFT_ERR_NO_DEVICE       -7
+#define PERFT_ERR_ILLEGAL_MOVE    -8
+#define PERFT_ERR_TIMEOUT         -9
+#define PERFT_ERR_NOT_FOUND      -10
+
+/* ---------------------------------------------------------------- types */
+
+/* Byte-compatible with HexaBitBoardPosition (chess.h:208-230):
+ * bb[0] white pieces, bb[1] pawns with packed state (bits 0-1 white
+ * castling, 2-3 black castling, 4-7 en-passant file + 1, 63 side to move),
+ * bb[2] knights, bb[3] bishops|queens, bb[4] rooks|queens, bb[5] kings. */
+typedef struct perft_pos48 {
+    uint64_t bb[6];
+} perft_pos48;
+
+/* Slider attack implementation (the reference's USE_SLIDING_LUT switch,
+ * switches.h:108-125, made a run-time choice). */
+#define PERFT_SLIDERS_AUTO   -1  /* autotuned per ply kind at init */
+#define PERFT_SLIDERS_KOGGE   0  /* Kogge-Stone occluded fills */
+#define PERFT_SLIDERS_MAGIC   1  /* fancy magic lookups */
+
+typedef struct perft_config {
+    int      device;          /* CUDA device ordinal */
+    uint64_t arena_bytes;     /* level-buffer budget in HBM; 0 = 85% of free */
+    int      sliders_expand;  /* PERFT_SLIDERS_* for interior plies */
+    int      sliders_leaf;    /* PERFT_SLIDERS_* for the count-only last ply */
+    int      tt_log2_entries; /* transposition table size; 0 = no table */
+    uint64_t zobrist_seed;    /* seed of the 781 Zobrist keys (TT only) */
+} perft_config;
+
+/* Defaults: device 0, automatic arena, autotuned sliders, no TT. */
+void perft_config_default(perft_config *cfg);
+
+/* Engine set-up: allocates the arena, uploads move-generator tables,
+ * autotunes.  Replaces initGPU + MoveGeneratorBitboard::init
+ * (launcher.h:1506-1533, MoveGeneratorBitboard.h:982-1201). */
+int perft_init(const perft_config *cfg);
+int perft_shutdown(void);
+const char *perft_status_string(int status);
+
+/* Leaf count of one position: perft_bb / perftLauncher
+ * (perft_bb.h:79-101, launcher.h:1455-1503), returned instead of printed. */
+int perft(const perft_pos48 *pos, uint32_t depth, uint64_t *out);
+
+/* Batched perft: out[i] = perft(pos[i], depths[i]).  Host buffers.
+ * Replaces the batch form of perft_bb_gpu_simple_hash (perft_bb.h:1242)
+ * used by perft_bb_last_level_launcher (launcher.h:966-1143) and the
+ * perft-records mode (launcher.h:1579-1695). */
+int perft_batch(const perft_pos48 *pos, const uint8_t *depths, uint32_t n, uint64_t *out);
+
+/* Same with positions and results already in device memory (depths stay on
+ * the host: they drive the launch plan).  Synchronous. */
+int perft_batch_device(const perft_pos48 *d_pos, const uint8_t *depths, uint32_t n,
+                       uint64_t *d_out);
+
+/* Divided perft: the legal moves of pos (UCI strings, 6 bytes each incl.
+ * NUL) and the perft(depth-1) of each child.  Replaces dividedPerft's
+ * per-move subtotals (launcher.h:1392-1450, 456-464). */
+int perft_divide(const perft_pos48 *pos, uint32_t depth, char (*moves)[6], uint64_t *counts,
+                 uint32_t *n_moves);
+
+/* ------------------------------------------------------- host utilities */
+
+/* FEN -> position: Utils::readFENString + board088ToHexBB
+ * (util.cpp:189-281, util.cpp:92-140).  Clocks are ignored; the en-passant
+ * square contributes its file only. */
+int perft_fen_to_pos(const char *fen, perft_pos48 *out);
+int perft_pos_to_fen(const perft_pos48 *pos, char *buf, size_t len);
+
+/* Legal moves in UCI notation, space separated (host move generator). */
+int perft_legal_moves_uci(const perft_pos48 *pos, char *buf, size_t len, uint32_t *n_moves);
+/* Applies one legal UCI move ("e2e4", "e7e8q"). */
+int perft_apply_uci_move(perft_pos48 *pos, const char *uci);
+
+/* Seeded random legal playouts from the initial position (std::mt19937_64,
+ * uniform move choice), rejecting positions without legal moves. */
+int perft_random_playouts(uint64_t seed, uint32_t n, uint32_t min_plies, uint32_t max_plies,
+                          perft_pos48 *out);
+
+/* Feature bits used to stratify synthetic workloads: 1 a legal en-passant
+ * capture exists, 2 the side to move has a pawn on its 7th rank, 4 a
+ * castling right remains, 8 the side to move is in check, 16 a promotion
+ * move exists. */
+int perft_position_features(const perft_pos48 *pos, uint32_t *features);
+
+/* ------------------------------------------------------------- statistics */
+typedef struct perft_stats {
+    uint64_t leaf_launches;      /* count-only tile kernel launches */
+    uint64_t expand_launches;    /* interior tile kernel launches */
+    uint64_t other_launches;     /* scan / init kernels */
+    uint64_t leaf_items;         /* (parent, move) pairs counted by leaf kernels */
+    uint64_t leaf_parents;       /* parents whose moves the leaf kernels generated */
+    uint64_t expand_items;       /* children written by interior kernels */
+    double   leaf_ms;            /* CUDA-event time of leaf kernels */
+    double   expand_ms;          /* CUDA-event time of interior kernels */
+    int      sliders_expand;     /* variant in use */
+    int      sliders_leaf;
+    uint64_t arena_bytes;
+    uint64_t peak_arena_bytes;
+    uint32_t chunked_levels;     /* levels split to fit the arena */
+} perft_stats;
+
+int perft_get_stats(perft_stats *out);
+int perft_reset_stats(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PERFT_B200_H */

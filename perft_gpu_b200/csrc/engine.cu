@@ -1,0 +1,818 @@
+// B200 perft engine: level-synchronous tree expansion with a fused,
+// count-only last ply.
+//
+// What it replaces in the reference (ankan-ban/perft_gpu):
+//   perft_bb_gpu_simple / _hash BFS drivers (perft_bb.h:1027-1138,
+//   1242-1589), the per-level kernels makemove_and_count_moves_single_level
+//   (perft_bb.h:601-625), generate_moves_single_level (perft_bb.h:983-996),
+//   the leaf pass makeMove_and_perft_single_level_indices (perft_bb.h:412-446)
+//   and moderngpu's ScanD + IntervalExpandDGenValues (perft_bb.h:1088-1124).
+//
+// Design (B200-first):
+//   * Boards are side-relative (movegen.cuh), so no kernel branches on the
+//     side to move.
+//   * A level is a structure-of-arrays buffer in HBM: six u64 planes plus
+//     the move count and root id of each node.  Every node of a level has
+//     the same remaining depth (roots are grouped by depth).
+//   * One exclusive scan of the move counts turns a level into a flat list
+//     of (parent, move) items.  Items are cut into fixed tiles of TILE_CAP;
+//     the scan also records the first parent of every tile, so the tile
+//     kernel needs no search and no parent-index expansion buffer.
+//   * The tile kernel is persistent (one wave of CTAs sized by occupancy)
+//     and steals tiles from an atomic counter.  Per tile it stages the
+//     parents in shared memory, generates their moves into a compact shared
+//     item list (only the moves inside the tile window), then every thread
+//     takes items: make the move, count the child's legal moves.  Interior
+//     plies write the child (coalesced: item order is child order) and its
+//     count; the last ply only sums counts per root, warp-aggregated with
+//     match/reduce before a shared-memory accumulator and one global atomic
+//     per root run.
+//   * When a level does not fit the HBM arena, its item range is split at
+//     tile boundaries and the chunks are expanded depth-first.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <stdio.h>
+#include <string.h>
+
+#include "../../include/perft_b200.h"
+#include "movegen.cuh"
+
+namespace pg {
+void build_tables();
+}  // namespace pg
+
+using namespace pg;
+
+namespace {
+
+// ------------------------------------------------------------- constants
+constexpr int TILE_NT = 256;
+constexpr int TILE_CAP_LOG2 = 12;
+constexpr int TILE_CAP = 1 << TILE_CAP_LOG2;
+constexpr int TILE_MAXP = TILE_NT;
+constexpr int MAX_LEGAL_MOVES = 218;
+
+constexpr int SCAN_NT = 512;
+constexpr int SCAN_IPT = 16;
+constexpr int SCAN_CHUNK = SCAN_NT * SCAN_IPT;
+constexpr int SCAN_TOP_NT = 1024;
+
+constexpr u32 DERR_GEN_MISMATCH = 1u;
+constexpr u32 DERR_BAD_ITEM = 2u;
+constexpr u32 DERR_BAD_POSITION = 4u;
+
+enum { MODE_EXPAND = 0, MODE_LEAF = 1 };
+
+// Bytes of one level node: 6 planes + count + root + scan entry.
+constexpr u64 NODE_BYTES = 6 * 8 + 4 + 4 + 8;
+
+// --------------------------------------------------------- block helpers
+template <int NT>
+__device__ __forceinline__ u64 block_excl_scan_u64(u64 v, u64 *sw, u64 &total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    u64 x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        u64 y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sw[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        u64 t = lane < NT / 32 ? sw[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            u64 y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < NT / 32) sw[lane] = t;
+    }
+    __syncthreads();
+    const u64 warpOff = w ? sw[w - 1] : 0;
+    total = sw[NT / 32 - 1];
+    __syncthreads();
+    return warpOff + x - v;
+}
+
+// Exclusive count of set flags over the block; total returned in *total.
+template <int NT>
+__device__ __forceinline__ int block_excl_count(bool flag, int *sw, int &total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned b = __ballot_sync(0xffffffffu, flag);
+    if (lane == 0) sw[w] = __popc(b);
+    __syncthreads();
+    int off = 0, tot = 0;
+#pragma unroll
+    for (int i = 0; i < NT / 32; i++) {
+        off += (i < w) ? sw[i] : 0;
+        tot += sw[i];
+    }
+    __syncthreads();
+    total = tot;
+    return off + __popc(b & ((1u << lane) - 1u));
+}
+
+// ------------------------------------------------------------------ scan
+// Exclusive scan of u32 move counts into u64 item offsets (n + 1 entries,
+// the last one the total), plus the first parent of every TILE_CAP tile.
+__global__ void __launch_bounds__(SCAN_NT) k_scan_reduce(const u32 *__restrict__ cnt, u64 n,
+                                                         u64 *__restrict__ bsum)
+{
+    __shared__ u64 sw[SCAN_NT / 32];
+    const u64 base = (u64)blockIdx.x * SCAN_CHUNK;
+    u64 s = 0;
+    for (int i = threadIdx.x; i < SCAN_CHUNK; i += SCAN_NT) {
+        const u64 k = base + i;
+        if (k < n) s += cnt[k];
+    }
+    u64 total;
+    block_excl_scan_u64<SCAN_NT>(s, sw, total);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SCAN_TOP_NT) k_scan_top(u64 *__restrict__ bsum, u64 nb,
+                                                          u64 *__restrict__ totalOut)
+{
+    __shared__ u64 sw[SCAN_TOP_NT / 32];
+    const u64 per = (nb + SCAN_TOP_NT - 1) / SCAN_TOP_NT;
+    const u64 b0 = per * threadIdx.x, b1 = min(b0 + per, nb);
+    u64 s = 0;
+    for (u64 i = b0; i < b1; i++) s += bsum[i];
+    u64 total;
+    u64 run = block_excl_scan_u64<SCAN_TOP_NT>(s, sw, total);
+    for (u64 i = b0; i < b1; i++) {
+        const u64 v = bsum[i];
+        bsum[i] = run;
+        run += v;
+    }
+    if (threadIdx.x == 0) *totalOut = total;
+}
+
+__global__ void __launch_bounds__(SCAN_NT) k_scan_apply(const u32 *__restrict__ cnt, u64 n,
+                                                        const u64 *__restrict__ bsum,
+                                                        u64 *__restrict__ scan,
+                                                        u32 *__restrict__ tileFirst)
+{
+    __shared__ u32 s[SCAN_CHUNK];
+    __shared__ u64 sw[SCAN_NT / 32];
+    const u64 base = (u64)blockIdx.x * SCAN_CHUNK;
+    for (int i = threadIdx.x; i < SCAN_CHUNK; i += SCAN_NT) {
+        const u64 k = base + i;
+        s[i] = k < n ? cnt[k] : 0u;
+    }
+    __syncthreads();
+    u64 local = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; k++) local += s[threadIdx.x * SCAN_IPT + k];
+    u64 total;
+    u64 run = bsum[blockIdx.x] + block_excl_scan_u64<SCAN_NT>(local, sw, total);
+    for (int k = 0; k < SCAN_IPT; k++) {
+        const u64 idx = base + (u64)threadIdx.x * SCAN_IPT + k;
+        if (idx >= n) break;
+        const u32 c = s[threadIdx.x * SCAN_IPT + k];
+        scan[idx] = run;
+        if (c) {
+            const u64 t0 = (run + TILE_CAP - 1) >> TILE_CAP_LOG2;
+            const u64 t1 = (run + c - 1) >> TILE_CAP_LOG2;
+            for (u64 t = t0; t <= t1; t++) tileFirst[t] = (u32)idx;
+        }
+        run += c;
+    }
+}
+
+// ----------------------------------------------------------------- roots
+__global__ void k_init_roots(const u64 *__restrict__ pos48, const u32 *__restrict__ ids, u32 n,
+                             u64 *__restrict__ planes, u64 stride, u32 *__restrict__ cnt,
+                             u32 *__restrict__ root, int depth,
+                             unsigned long long *__restrict__ rootCounts, u32 *err)
+{
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const u32 id = ids[i];
+    u64 p[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) p[k] = pos48[6 * (u64)id + k];
+    u32 c = 0;
+    Board b = from_pos48(p);
+    if (validate_pos48(p) != 0) {
+        atomicOr(err, DERR_BAD_POSITION);
+    } else {
+        c = count_moves<SV_KOGGE>(b);
+    }
+    planes[0 * stride + i] = b.mine;
+    planes[1 * stride + i] = b.pawns;
+    planes[2 * stride + i] = b.knights;
+    planes[3 * stride + i] = b.bq;
+    planes[4 * stride + i] = b.rq;
+    planes[5 * stride + i] = b.kings;
+    cnt[i] = c;
+    root[i] = id;
+    if (depth == 0) rootCounts[id] = 1ull;
+    if (depth == 1) rootCounts[id] = c;
+}
+
+// ------------------------------------------------------------ tile kernel
+struct TileParams {
+    const u64 *ppl;   // parent planes, plane i at ppl + i * pstride
+    u64 pstride;
+    const u64 *pscan; // nParents + 1 item offsets
+    const u32 *proot;
+    u64 nParents;
+    const u32 *tileFirst;  // indexed by absolute tile number
+    u64 itemBase;     // first item of this launch (multiple of TILE_CAP)
+    u64 itemEnd;      // one past the last item
+    u32 *tileCounter; // work-stealing cursor, zeroed before launch
+    // interior ply outputs (child index = item - itemBase)
+    u64 *cpl;
+    u64 cstride;
+    u32 *ccnt;
+    u32 *croot;
+    // last ply output
+    unsigned long long *rootCounts;
+    u32 *err;
+};
+
+// Emits a parent's moves, keeping only those whose global item index falls
+// inside [lo, hi): the window of the current tile.
+struct WindowSink {
+    u32 *items;
+    u64 g, lo, hi;
+    u32 tag;
+    __device__ __forceinline__ void operator()(u32 m)
+    {
+        if (g >= lo && g < hi) items[g - lo] = tag | m;
+        ++g;
+    }
+};
+
+template <int MODE, int SV>
+__global__ void __launch_bounds__(TILE_NT, 2) k_tile(const TileParams P)
+{
+    __shared__ u64 sb[6][TILE_MAXP];
+    __shared__ u32 sroot[TILE_MAXP];
+    __shared__ u32 srun[TILE_MAXP];
+    __shared__ u32 srunRoot[TILE_MAXP];
+    __shared__ unsigned long long sacc[TILE_MAXP];
+    __shared__ u32 sitems[TILE_CAP];
+    __shared__ int swarp[TILE_NT / 32];
+    __shared__ u32 sTile;
+
+    const int tid = threadIdx.x, lane = tid & 31;
+    const u64 tile0 = P.itemBase >> TILE_CAP_LOG2;
+    const u64 nTiles = (P.itemEnd - P.itemBase + TILE_CAP - 1) >> TILE_CAP_LOG2;
+
+    for (;;) {
+        if (tid == 0) sTile = atomicAdd(P.tileCounter, 1u);
+        __syncthreads();
+        const u64 tl = sTile;
+        if (tl >= nTiles) break;
+        const u64 iBeg = P.itemBase + (tl << TILE_CAP_LOG2);
+        const u64 iEnd = min(iBeg + (u64)TILE_CAP, P.itemEnd);
+        u64 p = P.tileFirst[tile0 + tl];
+
+        for (;;) {
+            // ---- stage the parents that own items of this window
+            const u64 q = p + tid;
+            u64 qBeg = 0, qEnd = 0;
+            bool valid = false;
+            if (q < P.nParents) {
+                qBeg = P.pscan[q];
+                valid = qBeg < iEnd;
+            }
+            const int nP = __syncthreads_count(valid);
+            if (valid) {
+                qEnd = P.pscan[q + 1];
+#pragma unroll
+                for (int k = 0; k < 6; k++) sb[k][tid] = P.ppl[k * P.pstride + q];
+                sroot[tid] = P.proot[q];
+            }
+            const u64 sBeg = max(P.pscan[p], iBeg);
+            const u64 sEnd = min(P.pscan[p + nP], iEnd);
+            __syncthreads();
+
+            int nRuns = 0;
+            if (MODE == MODE_LEAF) {
+                // parents are ordered by root: number the runs of equal roots
+                const bool head = valid && (tid == 0 || sroot[tid] != sroot[tid - 1]);
+                const int r = block_excl_count<TILE_NT>(head, swarp, nRuns);
+                if (valid) srun[tid] = head ? r : r - 1;
+                if (head) {
+                    srunRoot[r] = sroot[tid];
+                    sacc[r] = 0ull;
+                }
+            }
+
+            // ---- generate the window's moves into the shared item list
+            if (valid && qEnd > sBeg && qBeg < sEnd) {
+                const Board b{sb[0][tid], sb[1][tid], sb[2][tid], sb[3][tid], sb[4][tid], sb[5][tid]};
+                WindowSink sink{sitems, qBeg, sBeg, sEnd, (u32)tid << 16};
+                gen_moves<SV>(b, sink);
+                if (sink.g != qEnd) atomicOr(P.err, DERR_GEN_MISMATCH);
+            }
+            __syncthreads();
+
+            // ---- every thread takes items: make, count, write or sum
+            const int nItems = (int)(sEnd - sBeg);
+            for (int j0 = 0; j0 < nItems; j0 += TILE_NT) {
+                const int j = j0 + tid;
+                const bool act = j < nItems;
+                u32 cnt = 0;
+                int pl = 0;
+                if (act) {
+                    const u32 it = sitems[j];
+                    pl = (int)(it >> 16);
+                    if (pl < nP) {
+                        const Board b{sb[0][pl], sb[1][pl], sb[2][pl], sb[3][pl], sb[4][pl], sb[5][pl]};
+                        const Board ch = make_child(b, it & 0xFFFFu);
+                        cnt = count_moves<SV>(ch);
+                        if (MODE == MODE_EXPAND) {
+                            const u64 g = sBeg + (u64)j - P.itemBase;
+                            P.cpl[0 * P.cstride + g] = ch.mine;
+                            P.cpl[1 * P.cstride + g] = ch.pawns;
+                            P.cpl[2 * P.cstride + g] = ch.knights;
+                            P.cpl[3 * P.cstride + g] = ch.bq;
+                            P.cpl[4 * P.cstride + g] = ch.rq;
+                            P.cpl[5 * P.cstride + g] = ch.kings;
+                            P.ccnt[g] = cnt;
+                            P.croot[g] = sroot[pl];
+                        }
+                    } else {
+                        atomicOr(P.err, DERR_BAD_ITEM);
+                        pl = 0;
+                    }
+                }
+                if (MODE == MODE_LEAF) {
+                    const u32 key = act ? srun[pl] : 0xFFFFFFFFu;
+                    const unsigned peers = __match_any_sync(0xffffffffu, key);
+                    const u32 sum = __reduce_add_sync(peers, cnt);
+                    if (act && lane == __ffs(peers) - 1) atomicAdd(&sacc[key], (unsigned long long)sum);
+                }
+            }
+            __syncthreads();
+            if (MODE == MODE_LEAF && tid < nRuns) atomicAdd(&P.rootCounts[srunRoot[tid]], sacc[tid]);
+            if (sEnd >= iEnd || p + nP >= P.nParents) break;
+            p += nP;
+            __syncthreads();
+        }
+        __syncthreads();
+    }
+}
+
+// ================================================================ host side
+struct DeviceLevel {
+    u64 *planes;
+    u64 stride;
+    u32 *cnt;
+    u32 *root;
+    u64 n;
+};
+
+class Engine {
+public:
+    int init(const perft_config &cfg);
+    void shutdown();
+    int run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut);
+
+    perft_stats stats{};
+    std::mutex mu;
+    bool ready = false;
+    std::string lastCudaError;
+
+private:
+    int device = 0;
+    int nsm = 0;
+    cudaStream_t stream = nullptr;
+    char *arena = nullptr;
+    u64 arenaCap = 0, arenaTop = 0, arenaPeak = 0;
+    u32 *dCounter = nullptr;  // tile cursor
+    u32 *dErr = nullptr;
+    u64 *hPinned = nullptr;   // small read-backs
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int svExpand = SV_KOGGE, svLeaf = SV_KOGGE;
+    int gridTile[2][2] = {{0, 0}, {0, 0}};
+
+    void *alloc(u64 bytes)
+    {
+        const u64 a = (arenaTop + 255) & ~255ULL;
+        if (a + bytes > arenaCap) return nullptr;
+        arenaTop = a + bytes;
+        arenaPeak = std::max(arenaPeak, arenaTop);
+        return arena + a;
+    }
+    u64 arena_free() const { return arenaCap > arenaTop ? arenaCap - arenaTop : 0; }
+    bool alloc_level(DeviceLevel &L, u64 n);
+    int scan(const u32 *cnt, u64 n, u64 *&scanOut, u32 *&tileFirst, u64 &total);
+    int launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst,
+                    u64 itemBase, u64 itemEnd, DeviceLevel *children, unsigned long long *rootCounts);
+    int process_level(const DeviceLevel &L, int remaining, unsigned long long *rootCounts);
+    int check(cudaError_t e, const char *what);
+    int sync_and_check_errors();
+};
+
+int Engine::check(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return PERFT_OK;
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+    lastCudaError = buf;
+    return e == cudaErrorMemoryAllocation ? PERFT_ERR_OUT_OF_MEMORY : PERFT_ERR_CUDA;
+}
+
+#define ENG_TRY(expr)                                   \
+    do {                                                \
+        int rc_ = check((expr), #expr);                 \
+        if (rc_ != PERFT_OK) return rc_;                \
+    } while (0)
+
+template <int MODE, int SV>
+int occupancy_grid(int nsm)
+{
+    int perSm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_tile<MODE, SV>, TILE_NT, 0) != cudaSuccess ||
+        perSm < 1)
+        perSm = 1;
+    return perSm * nsm;
+}
+
+int Engine::init(const perft_config &cfg)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return PERFT_ERR_NO_DEVICE;
+    if (cfg.device < 0 || cfg.device >= ndev) return PERFT_ERR_INVALID_ARG;
+    device = cfg.device;
+    ENG_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    ENG_TRY(cudaGetDeviceProperties(&prop, device));
+    nsm = prop.multiProcessorCount;
+
+    build_tables();
+    ENG_TRY(cudaMemcpyToSymbol(d_tables, &h_tables, sizeof(Tables)));
+    ENG_TRY(cudaMemcpyToSymbol(d_magic, h_magic, sizeof(h_magic)));
+
+    // A blocking stream: it orders against the legacy default stream, where
+    // callers (and torch) usually produce device-resident inputs.
+    ENG_TRY(cudaStreamCreate(&stream));
+    ENG_TRY(cudaEventCreate(&ev0));
+    ENG_TRY(cudaEventCreate(&ev1));
+    ENG_TRY(cudaMalloc(&dCounter, 64));
+    ENG_TRY(cudaMalloc(&dErr, 64));
+    ENG_TRY(cudaMallocHost(&hPinned, 64));
+
+    size_t freeB = 0, totalB = 0;
+    ENG_TRY(cudaMemGetInfo(&freeB, &totalB));
+    u64 want = cfg.arena_bytes ? cfg.arena_bytes : (u64)(freeB * 0.85);
+    if (want > freeB) return PERFT_ERR_OUT_OF_MEMORY;
+    ENG_TRY(cudaMalloc(&arena, want));
+    arenaCap = want;
+
+    gridTile[MODE_EXPAND][SV_KOGGE] = occupancy_grid<MODE_EXPAND, SV_KOGGE>(nsm);
+    gridTile[MODE_EXPAND][SV_MAGIC] = occupancy_grid<MODE_EXPAND, SV_MAGIC>(nsm);
+    gridTile[MODE_LEAF][SV_KOGGE] = occupancy_grid<MODE_LEAF, SV_KOGGE>(nsm);
+    gridTile[MODE_LEAF][SV_MAGIC] = occupancy_grid<MODE_LEAF, SV_MAGIC>(nsm);
+
+    svExpand = cfg.sliders_expand == PERFT_SLIDERS_MAGIC ? SV_MAGIC : SV_KOGGE;
+    svLeaf = cfg.sliders_leaf == PERFT_SLIDERS_MAGIC ? SV_MAGIC : SV_KOGGE;
+    memset(&stats, 0, sizeof stats);
+    stats.sliders_expand = svExpand;
+    stats.sliders_leaf = svLeaf;
+    stats.arena_bytes = arenaCap;
+    ready = true;
+    return PERFT_OK;
+}
+
+void Engine::shutdown()
+{
+    if (!ready) return;
+    cudaSetDevice(device);
+    cudaStreamSynchronize(stream);
+    cudaFree(arena);
+    cudaFree(dCounter);
+    cudaFree(dErr);
+    cudaFreeHost(hPinned);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    cudaStreamDestroy(stream);
+    arena = nullptr;
+    ready = false;
+}
+
+bool Engine::alloc_level(DeviceLevel &L, u64 n)
+{
+    L.n = n;
+    L.stride = (n + 31) & ~31ULL;
+    L.planes = (u64 *)alloc(6 * 8 * L.stride);
+    L.cnt = (u32 *)alloc(4 * L.stride);
+    L.root = (u32 *)alloc(4 * L.stride);
+    return L.planes && L.cnt && L.root;
+}
+
+int Engine::scan(const u32 *cnt, u64 n, u64 *&scanOut, u32 *&tileFirst, u64 &total)
+{
+    const u64 nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    const u64 maxTiles = (n * MAX_LEGAL_MOVES + TILE_CAP - 1) / TILE_CAP + 1;
+    scanOut = (u64 *)alloc(8 * (n + 1));
+    tileFirst = (u32 *)alloc(4 * maxTiles);
+    u64 *bsum = (u64 *)alloc(8 * (nb + 1));
+    if (!scanOut || !tileFirst || !bsum) return PERFT_ERR_OUT_OF_MEMORY;
+    k_scan_reduce<<<(unsigned)nb, SCAN_NT, 0, stream>>>(cnt, n, bsum);
+    k_scan_top<<<1, SCAN_TOP_NT, 0, stream>>>(bsum, nb, scanOut + n);
+    k_scan_apply<<<(unsigned)nb, SCAN_NT, 0, stream>>>(cnt, n, bsum, scanOut, tileFirst);
+    stats.other_launches += 3;
+    ENG_TRY(cudaGetLastError());
+    ENG_TRY(cudaMemcpyAsync(hPinned, scanOut + n, 8, cudaMemcpyDeviceToHost, stream));
+    ENG_TRY(cudaStreamSynchronize(stream));
+    total = hPinned[0];
+    return PERFT_OK;
+}
+
+int Engine::launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst,
+                        u64 itemBase, u64 itemEnd, DeviceLevel *children,
+                        unsigned long long *rootCounts)
+{
+    TileParams P;
+    memset(&P, 0, sizeof P);
+    P.ppl = parents.planes;
+    P.pstride = parents.stride;
+    P.pscan = pscan;
+    P.proot = parents.root;
+    P.nParents = parents.n;
+    P.tileFirst = tileFirst;
+    P.itemBase = itemBase;
+    P.itemEnd = itemEnd;
+    P.tileCounter = dCounter;
+    if (children) {
+        P.cpl = children->planes;
+        P.cstride = children->stride;
+        P.ccnt = children->cnt;
+        P.croot = children->root;
+    }
+    P.rootCounts = rootCounts;
+    P.err = dErr;
+
+    const u64 nTiles = (itemEnd - itemBase + TILE_CAP - 1) / TILE_CAP;
+    const int sv = mode == MODE_LEAF ? svLeaf : svExpand;
+    const int grid = (int)std::min<u64>((u64)gridTile[mode][sv], nTiles);
+    ENG_TRY(cudaMemsetAsync(dCounter, 0, 4, stream));
+    ENG_TRY(cudaEventRecord(ev0, stream));
+    if (mode == MODE_LEAF) {
+        if (sv == SV_MAGIC) k_tile<MODE_LEAF, SV_MAGIC><<<grid, TILE_NT, 0, stream>>>(P);
+        else k_tile<MODE_LEAF, SV_KOGGE><<<grid, TILE_NT, 0, stream>>>(P);
+    } else {
+        if (sv == SV_MAGIC) k_tile<MODE_EXPAND, SV_MAGIC><<<grid, TILE_NT, 0, stream>>>(P);
+        else k_tile<MODE_EXPAND, SV_KOGGE><<<grid, TILE_NT, 0, stream>>>(P);
+    }
+    ENG_TRY(cudaGetLastError());
+    ENG_TRY(cudaEventRecord(ev1, stream));
+    ENG_TRY(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    ENG_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+    if (mode == MODE_LEAF) {
+        stats.leaf_launches++;
+        stats.leaf_items += itemEnd - itemBase;
+        stats.leaf_parents += parents.n;
+        stats.leaf_ms += ms;
+    } else {
+        stats.expand_launches++;
+        stats.expand_items += itemEnd - itemBase;
+        stats.expand_ms += ms;
+    }
+    return PERFT_OK;
+}
+
+// L holds the nodes of one level, all with `remaining` plies left (>= 2).
+int Engine::process_level(const DeviceLevel &L, int remaining, unsigned long long *rootCounts)
+{
+    if (L.n == 0) return PERFT_OK;
+    const u64 mark = arenaTop;
+    u64 *pscan = nullptr;
+    u32 *tileFirst = nullptr;
+    u64 total = 0;
+    int rc = scan(L.cnt, L.n, pscan, tileFirst, total);
+    if (rc != PERFT_OK) return rc;
+    if (total == 0) {
+        arenaTop = mark;
+        return PERFT_OK;
+    }
+    if (remaining == 2) {
+        rc = launch_tile(MODE_LEAF, L, pscan, tileFirst, 0, total, nullptr, rootCounts);
+        arenaTop = mark;
+        return rc;
+    }
+    // interior ply: children fit whole, or in tile-aligned chunks
+    const u64 slack = std::min<u64>(64ull << 20, arenaCap / 16);
+    const u64 freeB = arena_free() > slack ? arena_free() - slack : 0;
+    u64 budgetNodes = freeB / NODE_BYTES;
+    if (remaining > 3) budgetNodes /= 2;  // leave room for the plies below
+    u64 chunk = std::min<u64>(total, budgetNodes) & ~(u64)(TILE_CAP - 1);
+    if (chunk == 0) {
+        if (total <= budgetNodes) chunk = total;
+        else return PERFT_ERR_OUT_OF_MEMORY;
+    }
+    if (chunk < total) stats.chunked_levels++;
+    for (u64 lo = 0; lo < total; lo += chunk) {
+        const u64 hi = std::min(total, lo + chunk);
+        const u64 cm = arenaTop;
+        DeviceLevel C;
+        if (!alloc_level(C, hi - lo)) return PERFT_ERR_OUT_OF_MEMORY;
+        rc = launch_tile(MODE_EXPAND, L, pscan, tileFirst, lo, hi, &C, nullptr);
+        if (rc != PERFT_OK) return rc;
+        rc = process_level(C, remaining - 1, rootCounts);
+        if (rc != PERFT_OK) return rc;
+        arenaTop = cm;
+    }
+    arenaTop = mark;
+    return PERFT_OK;
+}
+
+int Engine::sync_and_check_errors()
+{
+    ENG_TRY(cudaMemcpyAsync(hPinned + 1, dErr, 4, cudaMemcpyDeviceToHost, stream));
+    ENG_TRY(cudaStreamSynchronize(stream));
+    const u32 e = (u32)hPinned[1];
+    if (e & DERR_BAD_POSITION) return PERFT_ERR_INVALID_ARG;
+    if (e) return PERFT_ERR_INTERNAL;
+    return PERFT_OK;
+}
+
+int Engine::run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut)
+{
+    ENG_TRY(cudaSetDevice(device));
+    const u64 mark0 = arenaTop;
+    unsigned long long *rootCounts = (unsigned long long *)dOut;
+    ENG_TRY(cudaMemsetAsync(rootCounts, 0, 8ull * n, stream));
+    ENG_TRY(cudaMemsetAsync(dErr, 0, 4, stream));
+
+    // group roots by depth: every node of a level then has the same remaining depth
+    std::map<int, std::vector<u32>, std::greater<int>> groups;
+    for (u32 i = 0; i < n; i++) groups[depths[i]].push_back(i);
+
+    int rc = PERFT_OK;
+    for (auto &g : groups) {
+        const int depth = g.first;
+        const std::vector<u32> &ids = g.second;
+        const u64 gm = arenaTop;
+        u32 *dIds = (u32 *)alloc(4ull * ids.size());
+        DeviceLevel L0;
+        if (!dIds || !alloc_level(L0, ids.size())) {
+            rc = PERFT_ERR_OUT_OF_MEMORY;
+            break;
+        }
+        ENG_TRY(cudaMemcpyAsync(dIds, ids.data(), 4ull * ids.size(), cudaMemcpyHostToDevice, stream));
+        const u32 nb = (u32)((ids.size() + 127) / 128);
+        k_init_roots<<<nb, 128, 0, stream>>>(dPos, dIds, (u32)ids.size(), L0.planes, L0.stride, L0.cnt,
+                                              L0.root, depth, rootCounts, dErr);
+        stats.other_launches++;
+        ENG_TRY(cudaGetLastError());
+        rc = sync_and_check_errors();
+        if (rc != PERFT_OK) break;
+        if (depth >= 2) rc = process_level(L0, depth, rootCounts);
+        arenaTop = gm;
+        if (rc != PERFT_OK) break;
+    }
+    arenaTop = mark0;
+    if (rc != PERFT_OK) {
+        cudaStreamSynchronize(stream);
+        return rc;
+    }
+    rc = sync_and_check_errors();
+    stats.peak_arena_bytes = std::max<u64>(stats.peak_arena_bytes, arenaPeak);
+    return rc;
+}
+
+// ================================================================ C ABI glue
+Engine g_engine;
+
+}  // namespace
+
+namespace pg {
+// Shared with host.cpp: run a batch on the process-wide engine (host buffers).
+int engine_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *out);
+}
+
+int pg::engine_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *out)
+{
+    Engine &E = g_engine;
+    std::lock_guard<std::mutex> lk(E.mu);
+    if (!E.ready) return PERFT_ERR_NOT_INITIALIZED;
+    if (n == 0) return PERFT_OK;
+    for (u32 i = 0; i < n; i++) {
+        if (validate_pos48(pos + 6ull * i) != 0) return PERFT_ERR_INVALID_ARG;
+        if (depths[i] > 20) return PERFT_ERR_INVALID_ARG;
+    }
+    u64 *dPos = nullptr, *dOut = nullptr;
+    if (cudaMalloc(&dPos, 48ull * n) != cudaSuccess) return PERFT_ERR_OUT_OF_MEMORY;
+    if (cudaMalloc(&dOut, 8ull * n) != cudaSuccess) {
+        cudaFree(dPos);
+        return PERFT_ERR_OUT_OF_MEMORY;
+    }
+    int rc = PERFT_OK;
+    if (cudaMemcpy(dPos, pos, 48ull * n, cudaMemcpyHostToDevice) != cudaSuccess) rc = PERFT_ERR_CUDA;
+    if (rc == PERFT_OK) rc = E.run_batch(dPos, depths, n, dOut);
+    if (rc == PERFT_OK && cudaMemcpy(out, dOut, 8ull * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = PERFT_ERR_CUDA;
+    cudaFree(dPos);
+    cudaFree(dOut);
+    return rc;
+}
+
+extern "C" {
+
+void perft_config_default(perft_config *cfg)
+{
+    if (!cfg) return;
+    memset(cfg, 0, sizeof *cfg);
+    cfg->device = 0;
+    cfg->arena_bytes = 0;
+    cfg->sliders_expand = PERFT_SLIDERS_AUTO;
+    cfg->sliders_leaf = PERFT_SLIDERS_AUTO;
+    cfg->tt_log2_entries = 0;
+    cfg->zobrist_seed = 0x5EED0781ULL;
+}
+
+int perft_init(const perft_config *cfg)
+{
+    perft_config c;
+    if (cfg) c = *cfg;
+    else perft_config_default(&c);
+    std::lock_guard<std::mutex> lk(g_engine.mu);
+    if (g_engine.ready) g_engine.shutdown();
+    return g_engine.init(c);
+}
+
+int perft_shutdown(void)
+{
+    std::lock_guard<std::mutex> lk(g_engine.mu);
+    g_engine.shutdown();
+    return PERFT_OK;
+}
+
+const char *perft_status_string(int status)
+{
+    switch (status) {
+    case PERFT_OK: return "ok";
+    case PERFT_ERR_INVALID_ARG: return "invalid argument";
+    case PERFT_ERR_NOT_INITIALIZED: return "engine not initialized (call perft_init)";
+    case PERFT_ERR_CUDA: return "CUDA error";
+    case PERFT_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case PERFT_ERR_INTERNAL: return "internal consistency check failed on the device";
+    case PERFT_ERR_BAD_FEN: return "malformed FEN";
+    case PERFT_ERR_NO_DEVICE: return "no CUDA device";
+    case PERFT_ERR_ILLEGAL_MOVE: return "illegal move";
+    case PERFT_ERR_TIMEOUT: return "timed out";
+    case PERFT_ERR_NOT_FOUND: return "not found";
+    default: return "unknown status";
+    }
+}
+
+int perft(const perft_pos48 *pos, uint32_t depth, uint64_t *out)
+{
+    if (!pos || !out || depth > 255) return PERFT_ERR_INVALID_ARG;
+    uint8_t d = (uint8_t)depth;
+    return pg::engine_batch_host(pos->bb, &d, 1, out);
+}
+
+int perft_batch(const perft_pos48 *pos, const uint8_t *depths, uint32_t n, uint64_t *out)
+{
+    if ((!pos || !depths || !out) && n) return PERFT_ERR_INVALID_ARG;
+    return pg::engine_batch_host(pos ? pos->bb : nullptr, depths, n, out);
+}
+
+int perft_batch_device(const perft_pos48 *d_pos, const uint8_t *depths, uint32_t n, uint64_t *d_out)
+{
+    if ((!d_pos || !depths || !d_out) && n) return PERFT_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_engine.mu);
+    if (!g_engine.ready) return PERFT_ERR_NOT_INITIALIZED;
+    for (u32 i = 0; i < n; i++)
+        if (depths[i] > 20) return PERFT_ERR_INVALID_ARG;
+    if (n == 0) return PERFT_OK;
+    return g_engine.run_batch(d_pos->bb, depths, n, d_out);
+}
+
+int perft_get_stats(perft_stats *out)
+{
+    if (!out) return PERFT_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_engine.mu);
+    *out = g_engine.stats;
+    return PERFT_OK;
+}
+
+int perft_reset_stats(void)
+{
+    std::lock_guard<std::mutex> lk(g_engine.mu);
+    perft_stats keep = g_engine.stats;
+    memset(&g_engine.stats, 0, sizeof g_engine.stats);
+    g_engine.stats.sliders_expand = keep.sliders_expand;
+    g_engine.stats.sliders_leaf = keep.sliders_leaf;
+    g_engine.stats.arena_bytes = keep.arena_bytes;
+    return PERFT_OK;
+}
+
+}  // extern "C"

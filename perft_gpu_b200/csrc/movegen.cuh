@@ -1,0 +1,802 @@
+// Side-relative bitboard move generator shared by the CUDA kernels and the
+// host utilities (FEN / UCI move parsing, position generators).
+//
+// Semantics follow the reference move generator (ankan-ban/perft_gpu,
+// MoveGeneratorBitboard.h): legal-move counting without generation
+// (countMoves :3008-3295, out of check :2828-3002), generation
+// (generateMoves :2471-2823, out of check :2269-2465) and make-move
+// (makeMove :3310-3570 with exact en-passant flagging, switches.h:48).
+//
+// Representation differs from the reference on purpose: every board is kept
+// from the point of view of the side to move ("mine" moves up the board).
+// A black-to-move position is stored vertically mirrored with colours
+// swapped.  Perft is invariant under that mirror, so counts are identical,
+// and the kernels need no per-side templates or side-dependent branches:
+// a warp whose lanes hold positions of different sides runs one code path.
+//
+// Board: six 64-bit planes, 48 bytes (same size and plane order as the
+// reference's HexaBitBoardPosition, chess.h:208-230, with "white pieces"
+// replaced by "pieces of the side to move"):
+//   mine, pawns, knights, bq (bishops|queens), rq (rooks|queens), kings
+// Pawns never stand on ranks 1/8, so the pawn plane carries the state:
+//   bits 0-1  castling rights of the side to move (1 king side, 2 queen side)
+//   bits 2-3  castling rights of the opponent
+//   bits 4-7  en-passant file + 1 (target on relative rank 6), 0 if none
+//   bit 63    1 when the real side to move is black
+// For a white-to-move position bits 0-7 coincide with the reference's packed
+// state byte.
+//
+// Moves are 16 bit: from (0-5), to (6-11), flags (12-15) with the
+// reference's CMove codes (chess.h:269-293).  Squares are relative.
+#pragma once
+
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define PG_HD __host__ __device__ __forceinline__
+#else
+#define PG_HD inline
+#endif
+
+namespace pg {
+
+typedef uint64_t u64;
+typedef uint32_t u32;
+
+struct Board {
+    u64 mine, pawns, knights, bq, rq, kings;
+};
+
+enum : u64 {
+    RANKS2TO7 = 0x00FFFFFFFFFFFF00ULL,
+    RANK1 = 0x00000000000000FFULL,
+    RANK3 = 0x0000000000FF0000ULL,
+    RANK5 = 0x000000FF00000000ULL,
+    RANK8 = 0xFF00000000000000ULL,
+    FILEA = 0x0101010101010101ULL,
+    FILEB = 0x0202020202020202ULL,
+    FILEG = 0x4040404040404040ULL,
+    FILEH = 0x8080808080808080ULL,
+    SIDE_BIT = 0x8000000000000000ULL,
+};
+
+enum : u32 {
+    MF_QUIET = 0,
+    MF_DOUBLE_PUSH = 1,
+    MF_KING_CASTLE = 2,
+    MF_QUEEN_CASTLE = 3,
+    MF_CAPTURE = 4,
+    MF_EP = 5,
+    MF_PROMO = 8,  // | 0 knight, 1 bishop, 2 rook, 3 queen; | 4 capture
+};
+
+// Slider attack implementation used by a kernel instantiation.
+enum SliderVariant : int {
+    SV_KOGGE = 0,   // occluded fills, all pieces of a set at once, no tables
+    SV_MAGIC = 1,   // fancy magic lookups, one per piece
+};
+
+// ------------------------------------------------------------------ tables
+// Built once on the host (tables.cpp) and copied to a __device__ symbol.
+struct Tables {
+    u64 king[64];
+    u64 knight[64];
+    u64 rookRays[64];    // empty-board rook attacks
+    u64 bishopRays[64];  // empty-board bishop attacks
+    u64 between[64][64]; // squares strictly between two squares on a line
+    u64 line[64][64];    // full line through two squares
+    u64 rookMask[64], bishopMask[64];
+    u64 rookMagic[64], bishopMagic[64];
+    u32 rookOffset[64], bishopOffset[64];
+    u32 rookShift[64], bishopShift[64];
+};
+
+// Total entries of the fancy-magic attack table (rook part then bishop part).
+constexpr u32 MAGIC_TABLE_ENTRIES = 102400 + 5248;
+
+extern Tables h_tables;
+extern u64 h_magic[MAGIC_TABLE_ENTRIES];
+
+#ifdef __CUDACC__
+// The one CUDA translation unit (engine.cu) defines the device copies.
+__device__ Tables d_tables;
+__device__ u64 d_magic[MAGIC_TABLE_ENTRIES];
+#endif
+
+#ifdef __CUDA_ARCH__
+#define PG_TAB(field) (__ldg(&d_tables.field))
+#define PG_MAGIC(i) (__ldg(&d_magic[(i)]))
+#else
+#define PG_TAB(field) (h_tables.field)
+#define PG_MAGIC(i) (h_magic[(i)])
+#endif
+
+// ------------------------------------------------------------- bit helpers
+PG_HD int popc(u64 x)
+{
+#ifdef __CUDA_ARCH__
+    return __popcll(x);
+#else
+    return __builtin_popcountll(x);
+#endif
+}
+
+PG_HD int ctz(u64 x)
+{
+#ifdef __CUDA_ARCH__
+    return __ffsll((long long)x) - 1;
+#else
+    return __builtin_ctzll(x);
+#endif
+}
+
+// Vertical mirror (rank r -> 7 - r): a byte swap.
+PG_HD u64 flipv(u64 x)
+{
+#ifdef __CUDA_ARCH__
+    u32 lo = (u32)x, hi = (u32)(x >> 32);
+    u32 nlo = __byte_perm(hi, 0, 0x0123);
+    u32 nhi = __byte_perm(lo, 0, 0x0123);
+    return ((u64)nhi << 32) | nlo;
+#else
+    return __builtin_bswap64(x);
+#endif
+}
+
+PG_HD u64 maskIf(bool c) { return (u64)0 - (u64)c; }
+
+// ------------------------------------------------------- one-square shifts
+PG_HD u64 sh_n(u64 x) { return x << 8; }
+PG_HD u64 sh_s(u64 x) { return x >> 8; }
+PG_HD u64 sh_e(u64 x) { return (x << 1) & ~FILEA; }
+PG_HD u64 sh_w(u64 x) { return (x >> 1) & ~FILEH; }
+PG_HD u64 sh_ne(u64 x) { return (x << 9) & ~FILEA; }
+PG_HD u64 sh_nw(u64 x) { return (x << 7) & ~FILEH; }
+PG_HD u64 sh_se(u64 x) { return (x >> 7) & ~FILEA; }
+PG_HD u64 sh_sw(u64 x) { return (x >> 9) & ~FILEH; }
+
+// ------------------------------------------------------------ Kogge-Stone
+// Occluded fill of generator set g through propagator p, then one more step:
+// every square attacked in that direction (first blocker included).  The
+// fill is OR-distributive over generators, and same-direction rays of
+// different pieces never share a non-own square, so per-direction popcounts
+// of a whole piece set sum to the per-piece move counts.
+template <int S, bool LEFT>
+PG_HD u64 ks_dir(u64 g, u64 p, u64 wrap)
+{
+    p &= wrap;
+    if (LEFT) {
+        g |= p & (g << S);
+        p &= p << S;
+        g |= p & (g << (2 * S));
+        p &= p << (2 * S);
+        g |= p & (g << (4 * S));
+        return (g << S) & wrap;
+    } else {
+        g |= p & (g >> S);
+        p &= p >> S;
+        g |= p & (g >> (2 * S));
+        p &= p >> (2 * S);
+        g |= p & (g >> (4 * S));
+        return (g >> S) & wrap;
+    }
+}
+
+PG_HD u64 ks_north(u64 g, u64 p) { return ks_dir<8, true>(g, p, ~0ULL); }
+PG_HD u64 ks_south(u64 g, u64 p) { return ks_dir<8, false>(g, p, ~0ULL); }
+PG_HD u64 ks_east(u64 g, u64 p) { return ks_dir<1, true>(g, p, ~FILEA); }
+PG_HD u64 ks_west(u64 g, u64 p) { return ks_dir<1, false>(g, p, ~FILEH); }
+PG_HD u64 ks_ne(u64 g, u64 p) { return ks_dir<9, true>(g, p, ~FILEA); }
+PG_HD u64 ks_nw(u64 g, u64 p) { return ks_dir<7, true>(g, p, ~FILEH); }
+PG_HD u64 ks_se(u64 g, u64 p) { return ks_dir<7, false>(g, p, ~FILEA); }
+PG_HD u64 ks_sw(u64 g, u64 p) { return ks_dir<9, false>(g, p, ~FILEH); }
+
+PG_HD u64 ks_diag(u64 g, u64 empty)
+{
+    return ks_ne(g, empty) | ks_nw(g, empty) | ks_se(g, empty) | ks_sw(g, empty);
+}
+PG_HD u64 ks_orth(u64 g, u64 empty)
+{
+    return ks_north(g, empty) | ks_south(g, empty) | ks_east(g, empty) | ks_west(g, empty);
+}
+
+// Per-direction move counts of a whole slider set (targets = squares the
+// pieces may land on).
+PG_HD int ks_count_diag(u64 g, u64 empty, u64 targets)
+{
+    return popc(ks_ne(g, empty) & targets) + popc(ks_nw(g, empty) & targets) +
+           popc(ks_se(g, empty) & targets) + popc(ks_sw(g, empty) & targets);
+}
+PG_HD int ks_count_orth(u64 g, u64 empty, u64 targets)
+{
+    return popc(ks_north(g, empty) & targets) + popc(ks_south(g, empty) & targets) +
+           popc(ks_east(g, empty) & targets) + popc(ks_west(g, empty) & targets);
+}
+
+// ------------------------------------------------------------------ magics
+PG_HD u64 magic_bishop(int sq, u64 occ)
+{
+    u64 idx = ((occ & PG_TAB(bishopMask[sq])) * PG_TAB(bishopMagic[sq])) >> PG_TAB(bishopShift[sq]);
+    return PG_MAGIC(PG_TAB(bishopOffset[sq]) + (u32)idx);
+}
+PG_HD u64 magic_rook(int sq, u64 occ)
+{
+    u64 idx = ((occ & PG_TAB(rookMask[sq])) * PG_TAB(rookMagic[sq])) >> PG_TAB(rookShift[sq]);
+    return PG_MAGIC(PG_TAB(rookOffset[sq]) + (u32)idx);
+}
+
+// Attacks of the piece on square sq given occupancy occ.
+template <int SV>
+PG_HD u64 bishop_att(int sq, u64 occ)
+{
+    if (SV == SV_MAGIC) return magic_bishop(sq, occ);
+    return ks_diag(1ULL << sq, ~occ);
+}
+template <int SV>
+PG_HD u64 rook_att(int sq, u64 occ)
+{
+    if (SV == SV_MAGIC) return magic_rook(sq, occ);
+    return ks_orth(1ULL << sq, ~occ);
+}
+
+// Union of the attacks of a slider set; occ excludes transparent squares.
+template <int SV>
+PG_HD u64 bishop_set_att(u64 set, u64 occ)
+{
+    if (SV == SV_KOGGE) return ks_diag(set, ~occ);
+    u64 a = 0;
+    while (set) {
+        a |= magic_bishop(ctz(set), occ);
+        set &= set - 1;
+    }
+    return a;
+}
+template <int SV>
+PG_HD u64 rook_set_att(u64 set, u64 occ)
+{
+    if (SV == SV_KOGGE) return ks_orth(set, ~occ);
+    u64 a = 0;
+    while (set) {
+        a |= magic_rook(ctz(set), occ);
+        set &= set - 1;
+    }
+    return a;
+}
+
+// ------------------------------------------------------------ leaper sets
+PG_HD u64 knight_set_att(u64 n)
+{
+    u64 l1 = (n >> 1) & 0x7f7f7f7f7f7f7f7fULL;
+    u64 l2 = (n >> 2) & 0x3f3f3f3f3f3f3f3fULL;
+    u64 r1 = (n << 1) & 0xfefefefefefefefeULL;
+    u64 r2 = (n << 2) & 0xfcfcfcfcfcfcfcfcULL;
+    u64 h1 = l1 | r1, h2 = l2 | r2;
+    return (h1 << 16) | (h1 >> 16) | (h2 << 8) | (h2 >> 8);
+}
+
+// Knight move count of a knight set by the eight (injective) jump shifts.
+PG_HD int knight_set_count(u64 n, u64 targets)
+{
+    const u64 notA = ~FILEA, notH = ~FILEH, notAB = ~(FILEA | FILEB), notGH = ~(FILEG | FILEH);
+    return popc((n << 17) & notA & targets) + popc((n << 15) & notH & targets) +
+           popc((n << 10) & notAB & targets) + popc((n << 6) & notGH & targets) +
+           popc((n >> 6) & notAB & targets) + popc((n >> 10) & notGH & targets) +
+           popc((n >> 15) & notA & targets) + popc((n >> 17) & notH & targets);
+}
+
+// Pawns of the side to move attack up, the opponent's attack down.
+PG_HD u64 pawn_att_up(u64 p) { return sh_ne(p) | sh_nw(p); }
+PG_HD u64 pawn_att_down(u64 p) { return sh_se(p) | sh_sw(p); }
+
+// ---------------------------------------------------------- position setup
+struct Ctx {
+    u64 pawns, occ, mine, theirs, empty;
+    u64 myK, tP, tN, tB, tR, tK;
+    u64 attacked;  // squares attacked by the opponent (own king transparent)
+    u32 st;        // state byte
+    int ksq;
+};
+
+template <int SV>
+PG_HD void setup_ctx(const Board &b, Ctx &c)
+{
+    c.pawns = b.pawns & RANKS2TO7;
+    c.occ = c.pawns | b.knights | b.bq | b.rq | b.kings;
+    c.mine = b.mine;
+    c.theirs = c.occ ^ b.mine;
+    c.empty = ~c.occ;
+    c.myK = b.kings & b.mine;
+    c.ksq = ctz(c.myK);
+    c.tP = c.pawns & c.theirs;
+    c.tN = b.knights & c.theirs;
+    c.tB = b.bq & c.theirs;
+    c.tR = b.rq & c.theirs;
+    c.tK = b.kings & c.theirs;
+    c.st = (u32)(b.pawns & 0xFF);
+    const u64 occNoK = c.occ ^ c.myK;
+    c.attacked = pawn_att_down(c.tP) | knight_set_att(c.tN) | PG_TAB(king[ctz(c.tK)]) |
+                 bishop_set_att<SV>(c.tB, occNoK) | rook_set_att<SV>(c.tR, occNoK);
+}
+
+// Checkers of the side to move's king.
+template <int SV>
+PG_HD u64 checkers_of(const Board &b, const Ctx &c)
+{
+    return (pawn_att_up(c.myK) & c.tP) | (PG_TAB(knight[c.ksq]) & c.tN) |
+           (bishop_att<SV>(c.ksq, c.occ) & c.tB) | (rook_att<SV>(c.ksq, c.occ) & c.tR);
+}
+
+// Pinned pieces of the side to move (findPinnedPieces, MoveGeneratorBitboard.h:1213-1249).
+PG_HD u64 pinned_of(const Ctx &c)
+{
+    u64 snipers = (PG_TAB(rookRays[c.ksq]) & c.tR) | (PG_TAB(bishopRays[c.ksq]) & c.tB);
+    u64 pinned = 0;
+    while (snipers) {
+        int s = ctz(snipers);
+        snipers &= snipers - 1;
+        u64 blk = PG_TAB(between[c.ksq][s]) & c.occ;
+        if (blk && !(blk & (blk - 1))) pinned |= blk & c.mine;
+    }
+    return pinned;
+}
+
+// Horizontal discovered-check test for an en-passant capture by an unpinned
+// pawn (MoveGeneratorBitboard.h:3079-3086): true when removing both pawns
+// exposes the king to a rook/queen along the rank.
+PG_HD bool ep_exposes_king(const Ctx &c, u64 src, u64 captured)
+{
+    if (!(c.myK & RANK5)) return false;
+    u64 pro = c.empty | src | captured;
+    return ((ks_east(c.myK, pro) | ks_west(c.myK, pro)) & c.tR) != 0;
+}
+
+// ------------------------------------------------------------------- count
+// Legal move count when in check (countMovesOutOfCheck).
+template <int SV>
+PG_HD u32 count_evasions(const Board &b, const Ctx &c)
+{
+    const u64 notMine = ~c.mine;
+    u32 n = popc(PG_TAB(king[c.ksq]) & notMine & ~c.attacked);
+    const u64 chk = checkers_of<SV>(b, c);
+    if (chk & (chk - 1)) return n;  // double check: king moves only
+    const int csq = ctz(chk);
+    const u64 safe = chk | PG_TAB(between[c.ksq][csq]);
+    const u64 pinned = pinned_of(c);
+    const u64 free = c.mine & ~pinned;
+
+    const u64 P = c.pawns & free;
+    const u64 p1 = sh_n(P) & c.empty;
+    const u64 p1s = p1 & safe;
+    n += popc(p1s) + 3 * popc(p1s & RANK8);
+    n += popc(sh_n(p1 & RANK3) & c.empty & safe);
+    const u64 cl = sh_nw(P) & chk, cr = sh_ne(P) & chk;
+    n += popc(cl) + popc(cr) + 3 * (popc(cl & RANK8) + popc(cr & RANK8));
+    const u32 epf = c.st >> 4;
+    if (epf) {
+        const u64 target = 1ULL << (39 + epf);
+        if (sh_s(target) == chk) n += popc(pawn_att_down(target) & P);
+    }
+
+    u64 N = b.knights & free;
+    while (N) {
+        n += popc(PG_TAB(knight[ctz(N)]) & safe);
+        N &= N - 1;
+    }
+    u64 B = b.bq & free;
+    while (B) {
+        n += popc(bishop_att<SV>(ctz(B), c.occ) & safe);
+        B &= B - 1;
+    }
+    u64 R = b.rq & free;
+    while (R) {
+        n += popc(rook_att<SV>(ctz(R), c.occ) & safe);
+        R &= R - 1;
+    }
+    return n;
+}
+
+// Legal move count of the side to move (countMoves).
+template <int SV>
+PG_HD u32 count_moves(const Board &b)
+{
+    Ctx c;
+    setup_ctx<SV>(b, c);
+    if (c.attacked & c.myK) return count_evasions<SV>(b, c);
+
+    const u64 notMine = ~c.mine;
+    u32 n = popc(PG_TAB(king[c.ksq]) & notMine & ~c.attacked);
+
+    // castling (relative squares: king e1, rooks h1/a1)
+    if ((c.st & 1) && !((c.occ | c.attacked) & 0x60ULL)) n++;
+    if ((c.st & 2) && !(c.occ & 0x0EULL) && !(c.attacked & 0x0CULL)) n++;
+
+    // pins: each pinned piece may only move along its pin line
+    u64 pinned = 0;
+    u64 snipers = (PG_TAB(rookRays[c.ksq]) & c.tR) | (PG_TAB(bishopRays[c.ksq]) & c.tB);
+    while (snipers) {
+        const int s = ctz(snipers);
+        snipers &= snipers - 1;
+        const u64 btw = PG_TAB(between[c.ksq][s]);
+        const u64 blk = btw & c.occ;
+        if (!blk || (blk & (blk - 1)) || !(blk & c.mine)) continue;
+        pinned |= blk;
+        const bool diag = (PG_TAB(bishopRays[c.ksq]) >> s) & 1;
+        if (blk & (diag ? b.bq : b.rq)) {
+            n += popc(btw);  // every square between king and pinner, minus its own, plus the capture
+        } else if (blk & c.pawns) {
+            if (diag) {
+                const u64 cap = pawn_att_up(blk) & (1ULL << s);
+                n += popc(cap) + 3 * popc(cap & RANK8);
+            } else if (((c.ksq ^ s) & 7) == 0) {
+                const u64 p1 = sh_n(blk) & c.empty;
+                n += popc(p1) + popc(sh_n(p1 & RANK3) & c.empty);
+            }
+        }
+    }
+
+    // free pawns, set-wise
+    const u64 P = c.pawns & c.mine & ~pinned;
+    const u64 p1 = sh_n(P) & c.empty;
+    n += popc(p1) + 3 * popc(p1 & RANK8);
+    n += popc(sh_n(p1 & RANK3) & c.empty);
+    const u64 cl = sh_nw(P) & c.theirs, cr = sh_ne(P) & c.theirs;
+    n += popc(cl) + popc(cr) + 3 * (popc(cl & RANK8) + popc(cr & RANK8));
+
+    // en passant
+    const u32 epf = c.st >> 4;
+    if (epf) {
+        const u64 target = 1ULL << (39 + epf);
+        const u64 captured = sh_s(target);
+        u64 srcs = pawn_att_down(target) & c.pawns & c.mine;
+        while (srcs) {
+            const u64 s = srcs & (0 - srcs);
+            srcs ^= s;
+            if (s & pinned) {
+                if (PG_TAB(line[ctz(s)][c.ksq]) & target) n++;
+            } else if (!ep_exposes_king(c, s, captured)) {
+                n++;
+            }
+        }
+    }
+
+    // knights
+    const u64 N = b.knights & c.mine & ~pinned;
+    if (SV == SV_KOGGE) {
+        n += knight_set_count(N, notMine);
+    } else {
+        u64 k = N;
+        while (k) {
+            n += popc(PG_TAB(knight[ctz(k)]) & notMine);
+            k &= k - 1;
+        }
+    }
+
+    // sliders
+    const u64 B = b.bq & c.mine & ~pinned;
+    const u64 R = b.rq & c.mine & ~pinned;
+    if (SV == SV_KOGGE) {
+        n += ks_count_diag(B, c.empty, notMine) + ks_count_orth(R, c.empty, notMine);
+    } else {
+        u64 x = B;
+        while (x) {
+            n += popc(magic_bishop(ctz(x), c.occ) & notMine);
+            x &= x - 1;
+        }
+        x = R;
+        while (x) {
+            n += popc(magic_rook(ctz(x), c.occ) & notMine);
+            x &= x - 1;
+        }
+    }
+    return n;
+}
+
+// ---------------------------------------------------------------- generate
+PG_HD u32 encode_move(int from, int to, u32 flags)
+{
+    return (flags << 12) | ((u32)to << 6) | (u32)from;
+}
+
+// Emits every target square of a piece as a move.
+template <class Sink>
+PG_HD void emit_targets(Sink &out, int from, u64 targets)
+{
+    while (targets) {
+        out(encode_move(from, ctz(targets), MF_QUIET));
+        targets &= targets - 1;
+    }
+}
+
+// Pawn move to dst with the four promotions on the last rank.
+template <class Sink>
+PG_HD void emit_pawn(Sink &out, int from, int to, u32 flags)
+{
+    if (to >= 56) {
+        out(encode_move(from, to, MF_PROMO | 0));
+        out(encode_move(from, to, MF_PROMO | 1));
+        out(encode_move(from, to, MF_PROMO | 2));
+        out(encode_move(from, to, MF_PROMO | 3));
+    } else {
+        out(encode_move(from, to, flags));
+    }
+}
+
+// Generates every legal move of the side to move.  Emits exactly
+// count_moves<SV>(b) moves.
+template <int SV, class Sink>
+PG_HD void gen_moves(const Board &b, Sink &out)
+{
+    Ctx c;
+    setup_ctx<SV>(b, c);
+    const u64 notMine = ~c.mine;
+    emit_targets(out, c.ksq, PG_TAB(king[c.ksq]) & notMine & ~c.attacked);
+
+    if (c.attacked & c.myK) {
+        const u64 chk = checkers_of<SV>(b, c);
+        if (chk & (chk - 1)) return;
+        const u64 safe = chk | PG_TAB(between[c.ksq][ctz(chk)]);
+        const u64 free = c.mine & ~pinned_of(c);
+        u64 P = c.pawns & free;
+        const u32 epf = c.st >> 4;
+        const u64 epTarget = epf ? (1ULL << (39 + epf)) : 0;
+        const bool epSaves = epf && sh_s(epTarget) == chk;
+        while (P) {
+            const int from = ctz(P);
+            const u64 p = P & (0 - P);
+            P ^= p;
+            const u64 p1 = sh_n(p) & c.empty;
+            if (p1 & safe) emit_pawn(out, from, from + 8, MF_QUIET);
+            const u64 p2 = sh_n(p1 & RANK3) & c.empty & safe;
+            if (p2) out(encode_move(from, from + 16, MF_DOUBLE_PUSH));
+            const u64 cap = pawn_att_up(p) & chk;
+            if (cap) emit_pawn(out, from, ctz(cap), MF_CAPTURE);
+            if (epSaves && (pawn_att_up(p) & epTarget)) out(encode_move(from, ctz(epTarget), MF_EP));
+        }
+        u64 N = b.knights & free;
+        while (N) {
+            const int s = ctz(N);
+            N &= N - 1;
+            emit_targets(out, s, PG_TAB(knight[s]) & safe);
+        }
+        u64 B = b.bq & free;
+        while (B) {
+            const int s = ctz(B);
+            B &= B - 1;
+            emit_targets(out, s, bishop_att<SV>(s, c.occ) & safe);
+        }
+        u64 R = b.rq & free;
+        while (R) {
+            const int s = ctz(R);
+            R &= R - 1;
+            emit_targets(out, s, rook_att<SV>(s, c.occ) & safe);
+        }
+        return;
+    }
+
+    if ((c.st & 1) && !((c.occ | c.attacked) & 0x60ULL)) out(encode_move(4, 6, MF_KING_CASTLE));
+    if ((c.st & 2) && !(c.occ & 0x0EULL) && !(c.attacked & 0x0CULL)) out(encode_move(4, 2, MF_QUEEN_CASTLE));
+
+    const u64 pinned = pinned_of(c);
+
+    // pinned pieces: along the pin line only
+    u64 pp = pinned;
+    while (pp) {
+        const int s = ctz(pp);
+        const u64 p = pp & (0 - pp);
+        pp ^= p;
+        const u64 line = PG_TAB(line[s][c.ksq]);
+        if (p & b.knights) continue;
+        if (p & c.pawns) {
+            const u64 p1 = sh_n(p) & c.empty & line;
+            if (p1) {
+                out(encode_move(s, s + 8, MF_QUIET));
+                if (sh_n(p1 & RANK3) & c.empty) out(encode_move(s, s + 16, MF_DOUBLE_PUSH));
+            }
+            const u64 cap = pawn_att_up(p) & line & c.theirs;
+            if (cap) emit_pawn(out, s, ctz(cap), MF_CAPTURE);
+            continue;
+        }
+        u64 t = 0;
+        if (p & b.bq) t |= bishop_att<SV>(s, c.occ);
+        if (p & b.rq) t |= rook_att<SV>(s, c.occ);
+        emit_targets(out, s, t & notMine & line);
+    }
+
+    // free pieces
+    u64 N = b.knights & c.mine & ~pinned;
+    while (N) {
+        const int s = ctz(N);
+        N &= N - 1;
+        emit_targets(out, s, PG_TAB(knight[s]) & notMine);
+    }
+    u64 B = b.bq & c.mine & ~pinned;
+    while (B) {
+        const int s = ctz(B);
+        B &= B - 1;
+        emit_targets(out, s, bishop_att<SV>(s, c.occ) & notMine);
+    }
+    u64 R = b.rq & c.mine & ~pinned;
+    while (R) {
+        const int s = ctz(R);
+        R &= R - 1;
+        emit_targets(out, s, rook_att<SV>(s, c.occ) & notMine);
+    }
+    const u64 P = c.pawns & c.mine & ~pinned;
+    u64 p1 = sh_n(P) & c.empty;
+    u64 p2 = sh_n(p1 & RANK3) & c.empty;
+    while (p1) {
+        const int to = ctz(p1);
+        p1 &= p1 - 1;
+        emit_pawn(out, to - 8, to, MF_QUIET);
+    }
+    while (p2) {
+        const int to = ctz(p2);
+        p2 &= p2 - 1;
+        out(encode_move(to - 16, to, MF_DOUBLE_PUSH));
+    }
+    u64 cl = sh_nw(P) & c.theirs;
+    while (cl) {
+        const int to = ctz(cl);
+        cl &= cl - 1;
+        emit_pawn(out, to - 7, to, MF_CAPTURE);
+    }
+    u64 cr = sh_ne(P) & c.theirs;
+    while (cr) {
+        const int to = ctz(cr);
+        cr &= cr - 1;
+        emit_pawn(out, to - 9, to, MF_CAPTURE);
+    }
+    const u32 epf = c.st >> 4;
+    if (epf) {
+        const u64 target = 1ULL << (39 + epf);
+        const u64 captured = sh_s(target);
+        u64 srcs = pawn_att_down(target) & c.pawns & c.mine;
+        while (srcs) {
+            const u64 s = srcs & (0 - srcs);
+            srcs ^= s;
+            bool ok = (s & pinned) ? ((PG_TAB(line[ctz(s)][c.ksq]) & target) != 0)
+                                   : !ep_exposes_king(c, s, captured);
+            if (ok) out(encode_move(ctz(s), 39 + epf, MF_EP));
+        }
+    }
+}
+
+// ------------------------------------------------------------------- make
+// Applies a legal move and returns the child from the opponent's point of
+// view (mirrored).  Branch-free except for the flag decode.
+PG_HD Board make_child(const Board &b, u32 mv)
+{
+    const int from = mv & 63, to = (mv >> 6) & 63;
+    const u32 fl = (mv >> 12) & 15;
+    const u64 src = 1ULL << from, dst = 1ULL << to, sd = src | dst;
+    const u64 st = b.pawns & 0xFF;
+    const u64 pawns0 = b.pawns & RANKS2TO7;
+    const u64 theirPawns = pawns0 & ~b.mine;
+
+    const u64 mP = maskIf((pawns0 >> from) & 1);
+    const u64 mN = maskIf((b.knights >> from) & 1);
+    const u64 mB = maskIf((b.bq >> from) & 1);
+    const u64 mR = maskIf((b.rq >> from) & 1);
+    const u64 mK = maskIf((b.kings >> from) & 1);
+
+    u64 pawns = pawns0 & ~sd;
+    u64 kn = b.knights & ~sd;
+    u64 bq = b.bq & ~sd;
+    u64 rq = b.rq & ~sd;
+    u64 kings = b.kings & ~src;
+
+    const u64 mPromo = maskIf(fl & 8);
+    const u32 pt = fl & 3;  // promotion piece: 0 N, 1 B, 2 R, 3 Q
+    pawns |= dst & mP & ~mPromo;
+    kn |= dst & ((mN & ~mPromo) | (mPromo & maskIf(pt == 0)));
+    bq |= dst & ((mB & ~mPromo) | (mPromo & maskIf(pt == 1 || pt == 3)));
+    rq |= dst & ((mR & ~mPromo) | (mPromo & maskIf(pt >= 2)));
+    kings |= dst & mK;
+
+    // en passant removes the pawn behind the target square
+    pawns &= ~(sh_s(dst) & maskIf(fl == MF_EP));
+    // castling moves the rook: h1->f1 or a1->d1
+    const u64 rookHop = (fl == MF_KING_CASTLE) ? 0xA0ULL : (fl == MF_QUEEN_CASTLE ? 0x09ULL : 0ULL);
+    rq ^= rookHop;
+    const u64 mine = ((b.mine & ~src) | dst) ^ rookHop;
+
+    // castling rights: king move, or anything leaving/landing on a rook corner
+    u64 clear = (mK & 3) | ((sd >> 7) & 1) | ((sd & 1) << 1) | ((sd >> 61) & 4) | ((sd >> 53) & 8);
+    const u64 st2 = st & ~clear;
+
+    // exact en-passant flagging: only when an enemy pawn stands beside dst
+    u64 epf = 0;
+    if (fl == MF_DOUBLE_PUSH && ((sh_e(dst) | sh_w(dst)) & theirPawns)) epf = (u64)((from & 7) + 1);
+
+    const u64 occ = pawns | kn | bq | rq | kings;
+    Board c;
+    c.mine = flipv(occ & ~mine);
+    c.pawns = flipv(pawns) | ((st2 >> 2) & 3) | ((st2 & 3) << 2) | (epf << 4) | ((~b.pawns) & SIDE_BIT);
+    c.knights = flipv(kn);
+    c.bq = flipv(bq);
+    c.rq = flipv(rq);
+    c.kings = flipv(kings);
+    return c;
+}
+
+// ---------------------------------------------------------- validation
+// 0 when a pos48 board is a position the generator can search: piece planes
+// disjoint (bishop and rook planes overlap only as queens), white pieces
+// within the occupancy, one king per side, en-passant file 0..8, and the
+// side not to move not in check.  The reference assumes all of this
+// (a missing king makes its bit scans undefined), so it is checked here.
+PG_HD int validate_pos48(const u64 p[6])
+{
+    const u64 pawns = p[1] & RANKS2TO7;
+    const u64 sl = p[3] | p[4];
+    const u64 occ = pawns | p[2] | sl | p[5];
+    if ((pawns & p[2]) | (pawns & sl) | (pawns & p[5]) | (p[2] & sl) | (p[2] & p[5]) | (p[5] & sl)) return 1;
+    if (p[0] & ~occ) return 2;
+    if (popc(p[5] & p[0]) != 1 || popc(p[5] & ~p[0]) != 1) return 3;
+    if (((p[1] >> 4) & 15) > 8) return 4;
+    // the opponent's king must not be capturable
+    const bool black = (p[1] >> 63) & 1;
+    const u64 mine = black ? (occ & ~p[0]) : p[0];
+    const u64 theirK = p[5] & ~mine;
+    const u64 myP = pawns & mine;
+    u64 att = (black ? pawn_att_down(myP) : pawn_att_up(myP)) | knight_set_att(p[2] & mine) |
+              ks_diag(p[3] & mine, ~occ) | ks_orth(p[4] & mine, ~occ);
+    const u64 k = p[5] & mine;
+    att |= sh_n(k) | sh_s(k) | sh_e(k) | sh_w(k) | sh_ne(k) | sh_nw(k) | sh_se(k) | sh_sw(k);
+    if (att & theirK) return 5;
+    return 0;
+}
+
+// -------------------------------------------------- absolute <-> relative
+// pos48: the reference's HexaBitBoardPosition (chess.h:208-230).
+PG_HD Board from_pos48(const u64 p[6])
+{
+    const u64 state = p[1];
+    const bool black = (state >> 63) & 1;
+    const u64 pawns = state & RANKS2TO7;
+    const u64 occ = pawns | p[2] | p[3] | p[4] | p[5];
+    const u64 wc = state & 3, bc = (state >> 2) & 3, ep = (state >> 4) & 15;
+    Board b;
+    if (!black) {
+        b.mine = p[0] & occ;
+        b.pawns = pawns | wc | (bc << 2) | (ep << 4);
+        b.knights = p[2];
+        b.bq = p[3];
+        b.rq = p[4];
+        b.kings = p[5];
+    } else {
+        b.mine = flipv(occ & ~p[0]);
+        b.pawns = flipv(pawns) | bc | (wc << 2) | (ep << 4) | SIDE_BIT;
+        b.knights = flipv(p[2]);
+        b.bq = flipv(p[3]);
+        b.rq = flipv(p[4]);
+        b.kings = flipv(p[5]);
+    }
+    return b;
+}
+
+PG_HD void to_pos48(const Board &b, u64 p[6])
+{
+    const bool black = (b.pawns >> 63) & 1;
+    const u64 st = b.pawns & 0xFF;
+    const u64 pawns = b.pawns & RANKS2TO7;
+    const u64 occ = pawns | b.knights | b.bq | b.rq | b.kings;
+    const u64 my = st & 3, their = (st >> 2) & 3, ep = (st >> 4) & 15;
+    if (!black) {
+        p[0] = b.mine;
+        p[1] = pawns | my | (their << 2) | (ep << 4);
+        p[2] = b.knights;
+        p[3] = b.bq;
+        p[4] = b.rq;
+        p[5] = b.kings;
+    } else {
+        p[0] = flipv(occ & ~b.mine);
+        p[1] = flipv(pawns) | their | (my << 2) | (ep << 4) | SIDE_BIT;
+        p[2] = flipv(b.knights);
+        p[3] = flipv(b.bq);
+        p[4] = flipv(b.rq);
+        p[5] = flipv(b.kings);
+    }
+}
+
+}  // namespace pg

@@ -1,0 +1,75 @@
+// Test-only: the product's move generator (perft_gpu_b200/csrc/movegen.cuh)
+// compiled for the host, so the CPU test suite can check it against the
+// oracle without a GPU.  Not part of the product library.
+#include <stdint.h>
+#include <string.h>
+
+#include "../../perft_gpu_b200/csrc/movegen.cuh"
+
+namespace pg {
+void build_tables();
+}
+
+using namespace pg;
+
+namespace {
+struct VecSink {
+    u32 *out;
+    u32 n;
+    void operator()(u32 m) { out[n++] = m; }
+};
+
+template <int SV>
+uint64_t perft_rel(const Board &b, uint32_t depth)
+{
+    if (depth == 0) return 1;
+    if (depth == 1) return count_moves<SV>(b);
+    u32 moves[256];
+    VecSink s{moves, 0};
+    gen_moves<SV>(b, s);
+    uint64_t total = 0;
+    for (u32 i = 0; i < s.n; i++) total += perft_rel<SV>(make_child(b, moves[i]), depth - 1);
+    return total;
+}
+}  // namespace
+
+extern "C" {
+
+int hc_init(void)
+{
+    build_tables();
+    return 0;
+}
+
+uint32_t hc_count(const uint64_t pos[6], int sv)
+{
+    Board b = from_pos48(pos);
+    return sv ? count_moves<SV_MAGIC>(b) : count_moves<SV_KOGGE>(b);
+}
+
+// Children of pos as pos48 boards; returns the number of moves.
+uint32_t hc_children(const uint64_t pos[6], int sv, uint64_t *out)
+{
+    Board b = from_pos48(pos);
+    u32 moves[256];
+    VecSink s{moves, 0};
+    if (sv) gen_moves<SV_MAGIC>(b, s);
+    else gen_moves<SV_KOGGE>(b, s);
+    for (u32 i = 0; i < s.n; i++) {
+        Board c = make_child(b, moves[i]);
+        to_pos48(c, out + 6 * i);
+    }
+    return s.n;
+}
+
+uint64_t hc_perft(const uint64_t pos[6], uint32_t depth, int sv)
+{
+    Board b = from_pos48(pos);
+    return sv ? perft_rel<SV_MAGIC>(b, depth) : perft_rel<SV_KOGGE>(b, depth);
+}
+
+void hc_roundtrip(const uint64_t pos[6], uint64_t out[6])
+{
+    to_pos48(from_pos48(pos), out);
+}
+}
