@@ -96,6 +96,27 @@ int perft_batch_device(const perft_pos48 *d_pos, const uint8_t *depths, uint32_t
 int perft_divide(const perft_pos48 *pos, uint32_t depth, char (*moves)[6], uint64_t *counts,
                  uint32_t *n_moves);
 
+/* Allocation-free batched perft.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory: processes whose HBM is
+ * already reserved by another allocator (a serving framework, torch's
+ * caching allocator), and latency-critical callers that cannot afford
+ * cudaMalloc's implicit device-wide synchronisation.  Same contract as
+ * perft_batch_device (device positions and results, host depths), plus the
+ * caller's stream (NULL = legacy default stream); needs no perft_init and
+ * allocates nothing: all working memory is one scratch array of
+ * PERFT_NOALLOC_SCRATCH_BYTES compiled into the library, which every GPU
+ * that loads the library keeps until the process exits.  Batches whose
+ * levels do not fit it fail with PERFT_ERR_OUT_OF_MEMORY (use the arena
+ * entry points for those).  All calls share the scratch; calls are
+ * serialised by a lock and return after their GPU work has finished, since
+ * overlapping calls would race on it.  The first call on a device uploads
+ * the move tables and looks up the scratch address; make it before any
+ * stream capture. */
+#define PERFT_NOALLOC_SCRATCH_BYTES (32ull << 20)
+int perft_batch_noalloc(const perft_pos48 *d_pos, const uint8_t *depths, uint32_t n,
+                        uint64_t *d_out, void *stream);
+
 /* ------------------------------------------------------- host utilities */
 
 /* FEN -> position: Utils::readFENString + board088ToHexBB

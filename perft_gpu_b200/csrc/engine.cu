@@ -816,3 +816,239 @@ int perft_reset_stats(void)
 }
 
 }  // extern "C"
+
+// ======================================================= allocation-free entry
+// perft_batch_noalloc: the batched perft for callers that cannot allocate
+// device memory — processes whose HBM is already reserved by another
+// allocator (a serving framework or torch's caching allocator holding the
+// device), and latency-critical callers for which cudaMalloc's implicit
+// device-wide synchronisation is unacceptable.  It runs the same kernels as
+// perft_batch_device, but every level buffer, scan, tile index and counter
+// lives in one fixed scratch array compiled into this library, so the call
+// allocates nothing.  Trees whose levels do not fit the scratch are refused
+// (PERFT_ERR_OUT_OF_MEMORY); the arena engine handles those by chunking.
+//
+// The scratch is a file-scope __device__ array: every GPU that loads this
+// library holds NOALLOC_SCRATCH_BYTES of it until the process exits.  All
+// calls on a device share it and it keeps the previous call's contents, so
+// each call clears its counters and outputs first.  Two calls whose GPU work
+// overlapped would corrupt each other: this entry point takes a process-wide
+// lock and waits for its work before returning, so its own calls never
+// overlap.  The first call on a device uploads the move-generator tables and
+// looks up the scratch address (cudaGetSymbolAddress) with that device
+// current; make that first call before any stream capture.
+static __device__ __align__(256) unsigned char g_noallocScratch[PERFT_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+struct NoallocDevice {
+    bool ready = false;
+    unsigned char *scratch = nullptr;  // device address of g_noallocScratch
+    int gridLeaf = 0, gridExpand = 0;
+};
+
+std::mutex g_noallocMu;
+NoallocDevice g_noallocDev[NOALLOC_MAX_DEVICES];
+
+// Writes, in order, the indices of the roots whose depth equals `depth`.
+__global__ void __launch_bounds__(1024) k_noalloc_group_ids(const uint8_t *__restrict__ depths, u32 n,
+                                                            int depth, u32 *__restrict__ ids,
+                                                            u32 *__restrict__ count)
+{
+    __shared__ int sw[32];
+    u32 base = 0;
+    for (u32 c0 = 0; c0 < n; c0 += 1024) {
+        const u32 i = c0 + threadIdx.x;
+        const bool hit = i < n && depths[i] == depth;
+        int tot = 0;
+        const int r = block_excl_count<1024>(hit, sw, tot);
+        if (hit) ids[base + r] = i;
+        base += (u32)tot;
+    }
+    if (threadIdx.x == 0) *count = base;
+}
+
+int noalloc_setup(int dev)
+{
+    NoallocDevice &D = g_noallocDev[dev];
+    if (D.ready) return PERFT_OK;
+    build_tables();
+    if (cudaMemcpyToSymbol(d_tables, &h_tables, sizeof(Tables)) != cudaSuccess) return PERFT_ERR_CUDA;
+    if (cudaMemcpyToSymbol(d_magic, h_magic, sizeof(h_magic)) != cudaSuccess) return PERFT_ERR_CUDA;
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noallocScratch) != cudaSuccess || p == nullptr) return PERFT_ERR_CUDA;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return PERFT_ERR_CUDA;
+    D.scratch = (unsigned char *)p;
+    D.gridLeaf = occupancy_grid<MODE_LEAF, SV_KOGGE>(prop.multiProcessorCount);
+    D.gridExpand = occupancy_grid<MODE_EXPAND, SV_KOGGE>(prop.multiProcessorCount);
+    D.ready = true;
+    return PERFT_OK;
+}
+
+// One call's bump allocator over the static scratch, and the level loop
+// without chunking.
+struct NoallocRun {
+    unsigned char *base;
+    u64 top = 0;
+    cudaStream_t st;
+    u32 *counter = nullptr, *err = nullptr;
+    int gridLeaf = 0, gridExpand = 0;
+
+    void *take(u64 bytes)
+    {
+        const u64 a = (top + 255) & ~255ULL;
+        if (a + bytes > PERFT_NOALLOC_SCRATCH_BYTES) return nullptr;
+        top = a + bytes;
+        return base + a;
+    }
+
+    bool level(DeviceLevel &L, u64 n)
+    {
+        L.n = n;
+        L.stride = (n + 31) & ~31ULL;
+        L.planes = (u64 *)take(6 * 8 * L.stride);
+        L.cnt = (u32 *)take(4 * L.stride);
+        L.root = (u32 *)take(4 * L.stride);
+        return L.planes && L.cnt && L.root;
+    }
+
+    int read_u64(const u64 *src, u64 &v)
+    {
+        if (cudaMemcpyAsync(&v, src, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess) return PERFT_ERR_CUDA;
+        return cudaStreamSynchronize(st) == cudaSuccess ? PERFT_OK : PERFT_ERR_CUDA;
+    }
+
+    int scan(const u32 *cnt, u64 n, u64 *&scanOut, u32 *&tileFirst, u64 &total)
+    {
+        const u64 nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+        const u64 maxTiles = (n * MAX_LEGAL_MOVES + TILE_CAP - 1) / TILE_CAP + 1;
+        scanOut = (u64 *)take(8 * (n + 1));
+        tileFirst = (u32 *)take(4 * maxTiles);
+        u64 *bsum = (u64 *)take(8 * (nb + 1));
+        if (!scanOut || !tileFirst || !bsum) return PERFT_ERR_OUT_OF_MEMORY;
+        k_scan_reduce<<<(unsigned)nb, SCAN_NT, 0, st>>>(cnt, n, bsum);
+        k_scan_top<<<1, SCAN_TOP_NT, 0, st>>>(bsum, nb, scanOut + n);
+        k_scan_apply<<<(unsigned)nb, SCAN_NT, 0, st>>>(cnt, n, bsum, scanOut, tileFirst);
+        if (cudaGetLastError() != cudaSuccess) return PERFT_ERR_CUDA;
+        return read_u64(scanOut + n, total);
+    }
+
+    int tile(int mode, const DeviceLevel &par, const u64 *pscan, const u32 *tileFirst, u64 total,
+             DeviceLevel *ch, unsigned long long *rootCounts)
+    {
+        TileParams P;
+        memset(&P, 0, sizeof P);
+        P.ppl = par.planes;
+        P.pstride = par.stride;
+        P.pscan = pscan;
+        P.proot = par.root;
+        P.nParents = par.n;
+        P.tileFirst = tileFirst;
+        P.itemBase = 0;
+        P.itemEnd = total;
+        P.tileCounter = counter;
+        if (ch) {
+            P.cpl = ch->planes;
+            P.cstride = ch->stride;
+            P.ccnt = ch->cnt;
+            P.croot = ch->root;
+        }
+        P.rootCounts = rootCounts;
+        P.err = err;
+        const u64 nTiles = (total + TILE_CAP - 1) / TILE_CAP;
+        if (cudaMemsetAsync(counter, 0, 4, st) != cudaSuccess) return PERFT_ERR_CUDA;
+        if (mode == MODE_LEAF)
+            k_tile<MODE_LEAF, SV_KOGGE><<<(int)std::min<u64>(gridLeaf, nTiles), TILE_NT, 0, st>>>(P);
+        else
+            k_tile<MODE_EXPAND, SV_KOGGE><<<(int)std::min<u64>(gridExpand, nTiles), TILE_NT, 0, st>>>(P);
+        return cudaGetLastError() == cudaSuccess ? PERFT_OK : PERFT_ERR_CUDA;
+    }
+
+    int process(const DeviceLevel &L, int remaining, unsigned long long *rootCounts)
+    {
+        if (L.n == 0) return PERFT_OK;
+        u64 *pscan = nullptr;
+        u32 *tileFirst = nullptr;
+        u64 total = 0;
+        int rc = scan(L.cnt, L.n, pscan, tileFirst, total);
+        if (rc != PERFT_OK || total == 0) return rc;
+        if (remaining == 2) return tile(MODE_LEAF, L, pscan, tileFirst, total, nullptr, rootCounts);
+        const u64 mark = top;
+        DeviceLevel C;
+        if (!level(C, total)) return PERFT_ERR_OUT_OF_MEMORY;
+        rc = tile(MODE_EXPAND, L, pscan, tileFirst, total, &C, nullptr);
+        if (rc == PERFT_OK) rc = process(C, remaining - 1, rootCounts);
+        top = mark;
+        return rc;
+    }
+};
+
+}  // namespace
+
+extern "C" int perft_batch_noalloc(const perft_pos48 *d_pos, const uint8_t *depths, uint32_t n,
+                                   uint64_t *d_out, void *stream)
+{
+    if ((!d_pos || !depths || !d_out) && n) return PERFT_ERR_INVALID_ARG;
+    for (uint32_t i = 0; i < n; i++)
+        if (depths[i] > 20) return PERFT_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_noallocMu);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PERFT_ERR_NO_DEVICE;
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return PERFT_ERR_INVALID_ARG;
+    int rc = noalloc_setup(dev);
+    if (rc != PERFT_OK || n == 0) return rc;
+
+    NoallocRun R;
+    R.base = g_noallocDev[dev].scratch;
+    R.st = (cudaStream_t)stream;
+    R.gridLeaf = g_noallocDev[dev].gridLeaf;
+    R.gridExpand = g_noallocDev[dev].gridExpand;
+    R.counter = (u32 *)R.take(4);
+    R.err = (u32 *)R.take(4);
+    u32 *dIds = (u32 *)R.take(4ull * n);
+    if (!R.counter || !R.err || !dIds) return PERFT_ERR_OUT_OF_MEMORY;
+    unsigned long long *rootCounts = (unsigned long long *)d_out;
+    if (cudaMemsetAsync(R.err, 0, 4, R.st) != cudaSuccess) return PERFT_ERR_CUDA;
+    if (cudaMemsetAsync(rootCounts, 0, 8ull * n, R.st) != cudaSuccess) return PERFT_ERR_CUDA;
+
+    // Group roots by depth without host allocation: the depths go to the
+    // scratch and a kernel compacts the ids of one depth group in order.
+    u32 perDepth[21] = {0};
+    for (u32 i = 0; i < n; i++) perDepth[depths[i]]++;
+    uint8_t *dDepths = (uint8_t *)R.take(n);
+    u32 *dGroupCount = (u32 *)R.take(4);
+    if (!dDepths || !dGroupCount) return PERFT_ERR_OUT_OF_MEMORY;
+    if (cudaMemcpyAsync(dDepths, depths, n, cudaMemcpyHostToDevice, R.st) != cudaSuccess)
+        return PERFT_ERR_CUDA;
+
+    for (int depth = 20; depth >= 0; depth--) {
+        const u32 cnt = perDepth[depth];
+        if (!cnt) continue;
+        const u64 mark = R.top;
+        DeviceLevel L0;
+        if (!R.level(L0, cnt)) {
+            rc = PERFT_ERR_OUT_OF_MEMORY;
+            break;
+        }
+        k_noalloc_group_ids<<<1, 1024, 0, R.st>>>(dDepths, n, depth, dIds, dGroupCount);
+        k_init_roots<<<(cnt + 127) / 128, 128, 0, R.st>>>(d_pos->bb, dIds, cnt, L0.planes, L0.stride,
+                                                           L0.cnt, L0.root, depth, rootCounts, R.err);
+        if (cudaGetLastError() != cudaSuccess) {
+            rc = PERFT_ERR_CUDA;
+            break;
+        }
+        if (depth >= 2) rc = R.process(L0, depth, rootCounts);
+        R.top = mark;
+        if (rc != PERFT_OK) break;
+    }
+    u32 e = 0;
+    if (cudaMemcpyAsync(&e, R.err, 4, cudaMemcpyDeviceToHost, R.st) != cudaSuccess ||
+        cudaStreamSynchronize(R.st) != cudaSuccess)
+        return PERFT_ERR_CUDA;
+    if (rc != PERFT_OK) return rc;
+    if (e & DERR_BAD_POSITION) return PERFT_ERR_INVALID_ARG;
+    return e ? PERFT_ERR_INTERNAL : PERFT_OK;
+}
