@@ -108,10 +108,10 @@ def load_work_figures():
 def int32_peak(device):
     """Measured integer-pipe peak (ops/s) from libperft_probe.so."""
     lib = ctypes.CDLL(os.path.join(ROOT, "perft_gpu_b200", "libperft_probe.so"))
-    out = (ctypes.c_double * 4)()
+    out = (ctypes.c_double * 5)()
     if lib.perft_int32_peak_probe(device, out) != 0:
         return None
-    return {"lop3": out[0], "iadd3": out[1], "mix": out[2], "imad": out[3]}
+    return {"lop3": out[0], "iadd": out[1], "lop3_iadd_shf": out[2], "imad": out[3], "lop3_imad": out[4]}
 
 
 def traffic_from_profiles(workload):
@@ -124,13 +124,14 @@ def traffic_from_profiles(workload):
 
 
 # ------------------------------------------------------------------ workloads
-def make_workload(name, rank):
+def make_workload(name, rank, positions=4096):
     from perft_gpu_b200 import workloads as W
     if name == "batch":
         pos, depths = W.batch_positions(n=4096, seed=2026 + rank)
-        cfg = {"workload": "batch4096: 4096 seeded playouts of 8-30 plies, stratified "
+        pos, depths = pos[:positions], depths[:positions]
+        cfg = {"workload": f"batch{positions}: {positions} seeded playouts of 8-30 plies, stratified "
                            "(>=10% en passant, >=10% pawn on 7th, >=10% castling), depth U[4,6]",
-               "positions": 4096, "depths": "U[4,6]", "seed": 2026 + rank}
+               "positions": positions, "depths": "U[4,6]", "seed": 2026 + rank}
         return pos, depths, cfg, "batch4096"
     if name == "start":
         pos = np.repeat(W.start_position().reshape(1, 6), 1, axis=0)
@@ -183,7 +184,7 @@ def cpu_sample(pos, depths, budget_s, expected=None, threads=None):
             mismatches += int(np.count_nonzero(out != expected[idx]))
         leaves += int(out.sum())
         done += len(idx)
-        group = min(group * 2, 512)
+        group = min(group * 2, 128)
     el = time.perf_counter() - t0
     return {"value": leaves / el, "unit": UNIT, "cores": threads, "kind": kind,
             "sample": f"{done} of {len(pos)} positions (seeded order) at their own depths, "
@@ -195,7 +196,7 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    pos, depths, cfg, _ = make_workload(args.workload, 0)
+    pos, depths, cfg, _ = make_workload(args.workload, 0, args.positions)
     vals = []
     for _ in range(args.warmup):
         cpu_sample(pos, depths, min(3.0, args.cpu_seconds))
@@ -229,9 +230,10 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
 
-    pos, depths, cfg, wf_key = make_workload(args.workload, rank)
-    sliders = {"auto": pg.SLIDERS_AUTO, "kogge": pg.SLIDERS_KOGGE, "magic": pg.SLIDERS_MAGIC}[args.sliders]
-    pg.init(device=local, sliders_expand=sliders, sliders_leaf=sliders)
+    pos, depths, cfg, wf_key = make_workload(args.workload, rank, args.positions)
+    sliders = {"auto": pg.SLIDERS_AUTO, **{v: k for k, v in pg.SLIDER_NAMES.items()}}[args.sliders]
+    pg.init(device=local, sliders_expand=sliders, sliders_leaf=sliders,
+            arena_bytes=int(args.arena_gb * (1 << 30)))
 
     n = len(pos)
     d_pos = torch.from_numpy(pos.view(np.int64)).cuda()
@@ -302,7 +304,7 @@ def run_ours(args):
     w_int = 2.0 * (st["leaf_items"] * (wf["c_make"] + wf["c_count"]) + st["leaf_parents"] * wf["c_gen"])
     leaf_s = st["leaf_ms"] / 1e3
     achieved = w_int / leaf_s if leaf_s > 0 else None
-    peak = peaks["mix"] if peaks else None
+    peak = max(peaks.values()) if peaks else None
     roofline = {
         "bound": "int32",
         "kernel": "k_tile<MODE_LEAF> (count-only last ply)",
@@ -310,7 +312,7 @@ def run_ours(args):
         "peak": peak / 1e12 if peak else None,
         "unit": "Tops/s (32-bit integer ops, reference-algorithm work)",
         "frac": (achieved / peak) if (achieved and peak) else None,
-        "peak_source": "measured on this GPU by libperft_probe.so (LOP3+IADD3+SHF stream), of measured",
+        "peak_source": "of measured: best of the integer instruction mixes timed on this GPU by libperft_probe.so",
         "peak_variants_tops": {k: v / 1e12 for k, v in peaks.items()} if peaks else None,
         "traffic": traffic_from_profiles(wf_key),
         "work_per_launch_ops": w_int / launches,
@@ -324,7 +326,9 @@ def run_ours(args):
         cpu = cpu_sample(pos, depths, args.cpu_seconds, expected=counts)
 
     cfg = dict(cfg)
-    cfg.update({"sliders": {0: "kogge", 1: "magic"}.get(st["sliders_leaf"], "?"),
+    cfg.update({"sliders": {"leaf": pg.SLIDER_NAMES.get(st["sliders_leaf"], "?"),
+                            "interior": pg.SLIDER_NAMES.get(st["sliders_expand"], "?"),
+                            "chosen_by": args.sliders},
                 "l2": "no flush: each step streams multi-GB level buffers through HBM (>> 126 MB L2)",
                 "parallelism": f"independent batches, {ws} GPU(s)"})
     line = {
@@ -352,7 +356,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["batch", "start", "deep"], default="batch")
-    ap.add_argument("--sliders", choices=["auto", "kogge", "magic"], default="auto")
+    ap.add_argument("--sliders", choices=["auto", "kogge", "magic", "kogge_fma", "kogge_mix"], default="auto")
+    ap.add_argument("--positions", type=int, default=4096,
+                    help="batch workload: use the first N positions (profiling runs)")
+    ap.add_argument("--arena-gb", type=float, default=0.0, help="level-buffer arena (0 = 85%% of free HBM)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()

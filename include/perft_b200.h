@@ -52,9 +52,11 @@ typedef struct perft_pos48 {
 
 /* Slider attack implementation (the reference's USE_SLIDING_LUT switch,
  * switches.h:108-125, made a run-time choice). */
-#define PERFT_SLIDERS_AUTO   -1  /* autotuned per ply kind at init */
-#define PERFT_SLIDERS_KOGGE   0  /* Kogge-Stone occluded fills */
-#define PERFT_SLIDERS_MAGIC   1  /* fancy magic lookups */
+#define PERFT_SLIDERS_AUTO      -1  /* autotuned per ply kind at init */
+#define PERFT_SLIDERS_KOGGE      0  /* Kogge-Stone occluded fills */
+#define PERFT_SLIDERS_MAGIC      1  /* fancy magic lookups */
+#define PERFT_SLIDERS_KOGGE_FMA  2  /* Kogge-Stone, constant shifts on the FMA pipe */
+#define PERFT_SLIDERS_KOGGE_MIX  3  /* Kogge-Stone, FMA-pipe shifts for attack maps only */
 
 typedef struct perft_config {
     int      device;          /* CUDA device ordinal */

@@ -36,6 +36,10 @@ PERFT_ERR_NOT_FOUND = -10
 SLIDERS_AUTO = -1
 SLIDERS_KOGGE = 0
 SLIDERS_MAGIC = 1
+SLIDERS_KOGGE_FMA = 2
+SLIDERS_KOGGE_MIX = 3
+SLIDER_NAMES = {SLIDERS_KOGGE: "kogge", SLIDERS_MAGIC: "magic", SLIDERS_KOGGE_FMA: "kogge_fma",
+                SLIDERS_KOGGE_MIX: "kogge_mix"}
 
 START_FEN = "rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1"
 

@@ -397,7 +397,7 @@ private:
     u64 *hPinned = nullptr;   // small read-backs
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int svExpand = SV_KOGGE, svLeaf = SV_KOGGE;
-    int gridTile[2][2] = {{0, 0}, {0, 0}};
+    int gridTile[2][SV_COUNT] = {};
 
     void *alloc(u64 bytes)
     {
@@ -415,6 +415,7 @@ private:
     int process_level(const DeviceLevel &L, int remaining, unsigned long long *rootCounts);
     int check(cudaError_t e, const char *what);
     int sync_and_check_errors();
+    int autotune(bool leaf, bool expand);
 };
 
 int Engine::check(cudaError_t e, const char *what)
@@ -442,6 +443,28 @@ int occupancy_grid(int nsm)
     return perSm * nsm;
 }
 
+template <int MODE>
+void launch_tile_variant(int sv, int grid, cudaStream_t st, const TileParams &P)
+{
+    switch (sv) {
+    case SV_MAGIC: k_tile<MODE, SV_MAGIC><<<grid, TILE_NT, 0, st>>>(P); break;
+    case SV_KOGGE_FMA: k_tile<MODE, SV_KOGGE_FMA><<<grid, TILE_NT, 0, st>>>(P); break;
+    case SV_KOGGE_MIX: k_tile<MODE, SV_KOGGE_MIX><<<grid, TILE_NT, 0, st>>>(P); break;
+    default: k_tile<MODE, SV_KOGGE><<<grid, TILE_NT, 0, st>>>(P); break;
+    }
+}
+
+const char *slider_name(int sv)
+{
+    switch (sv) {
+    case SV_KOGGE: return "kogge";
+    case SV_MAGIC: return "magic";
+    case SV_KOGGE_FMA: return "kogge_fma";
+    case SV_KOGGE_MIX: return "kogge_mix";
+    default: return "?";
+    }
+}
+
 int Engine::init(const perft_config &cfg)
 {
     int ndev = 0;
@@ -456,6 +479,9 @@ int Engine::init(const perft_config &cfg)
     build_tables();
     ENG_TRY(cudaMemcpyToSymbol(d_tables, &h_tables, sizeof(Tables)));
     ENG_TRY(cudaMemcpyToSymbol(d_magic, h_magic, sizeof(h_magic)));
+    u32 pow2[32];
+    for (int k = 0; k < 32; k++) pow2[k] = 1u << k;
+    ENG_TRY(cudaMemcpyToSymbol(c_pow2, pow2, sizeof pow2));
 
     // A blocking stream: it orders against the legacy default stream, where
     // callers (and torch) usually produce device-resident inputs.
@@ -475,16 +501,30 @@ int Engine::init(const perft_config &cfg)
 
     gridTile[MODE_EXPAND][SV_KOGGE] = occupancy_grid<MODE_EXPAND, SV_KOGGE>(nsm);
     gridTile[MODE_EXPAND][SV_MAGIC] = occupancy_grid<MODE_EXPAND, SV_MAGIC>(nsm);
+    gridTile[MODE_EXPAND][SV_KOGGE_FMA] = occupancy_grid<MODE_EXPAND, SV_KOGGE_FMA>(nsm);
+    gridTile[MODE_EXPAND][SV_KOGGE_MIX] = occupancy_grid<MODE_EXPAND, SV_KOGGE_MIX>(nsm);
     gridTile[MODE_LEAF][SV_KOGGE] = occupancy_grid<MODE_LEAF, SV_KOGGE>(nsm);
     gridTile[MODE_LEAF][SV_MAGIC] = occupancy_grid<MODE_LEAF, SV_MAGIC>(nsm);
+    gridTile[MODE_LEAF][SV_KOGGE_FMA] = occupancy_grid<MODE_LEAF, SV_KOGGE_FMA>(nsm);
+    gridTile[MODE_LEAF][SV_KOGGE_MIX] = occupancy_grid<MODE_LEAF, SV_KOGGE_MIX>(nsm);
 
-    svExpand = cfg.sliders_expand == PERFT_SLIDERS_MAGIC ? SV_MAGIC : SV_KOGGE;
-    svLeaf = cfg.sliders_leaf == PERFT_SLIDERS_MAGIC ? SV_MAGIC : SV_KOGGE;
+    auto pick = [](int v) { return (v >= 0 && v < SV_COUNT) ? v : SV_KOGGE; };
+    svExpand = pick(cfg.sliders_expand);
+    svLeaf = pick(cfg.sliders_leaf);
+    ready = true;
+    const bool tuneLeaf = cfg.sliders_leaf == PERFT_SLIDERS_AUTO;
+    const bool tuneExpand = cfg.sliders_expand == PERFT_SLIDERS_AUTO;
+    if (tuneLeaf || tuneExpand) {
+        const int rc = autotune(tuneLeaf, tuneExpand);
+        if (rc != PERFT_OK) {
+            ready = false;
+            return rc;
+        }
+    }
     memset(&stats, 0, sizeof stats);
     stats.sliders_expand = svExpand;
     stats.sliders_leaf = svLeaf;
     stats.arena_bytes = arenaCap;
-    ready = true;
     return PERFT_OK;
 }
 
@@ -562,13 +602,8 @@ int Engine::launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, 
     const int grid = (int)std::min<u64>((u64)gridTile[mode][sv], nTiles);
     ENG_TRY(cudaMemsetAsync(dCounter, 0, 4, stream));
     ENG_TRY(cudaEventRecord(ev0, stream));
-    if (mode == MODE_LEAF) {
-        if (sv == SV_MAGIC) k_tile<MODE_LEAF, SV_MAGIC><<<grid, TILE_NT, 0, stream>>>(P);
-        else k_tile<MODE_LEAF, SV_KOGGE><<<grid, TILE_NT, 0, stream>>>(P);
-    } else {
-        if (sv == SV_MAGIC) k_tile<MODE_EXPAND, SV_MAGIC><<<grid, TILE_NT, 0, stream>>>(P);
-        else k_tile<MODE_EXPAND, SV_KOGGE><<<grid, TILE_NT, 0, stream>>>(P);
-    }
+    if (mode == MODE_LEAF) launch_tile_variant<MODE_LEAF>(sv, grid, stream, P);
+    else launch_tile_variant<MODE_EXPAND>(sv, grid, stream, P);
     ENG_TRY(cudaGetLastError());
     ENG_TRY(cudaEventRecord(ev1, stream));
     ENG_TRY(cudaEventSynchronize(ev1));
@@ -611,11 +646,9 @@ int Engine::process_level(const DeviceLevel &L, int remaining, unsigned long lon
     const u64 freeB = arena_free() > slack ? arena_free() - slack : 0;
     u64 budgetNodes = freeB / NODE_BYTES;
     if (remaining > 3) budgetNodes /= 2;  // leave room for the plies below
-    u64 chunk = std::min<u64>(total, budgetNodes) & ~(u64)(TILE_CAP - 1);
-    if (chunk == 0) {
-        if (total <= budgetNodes) chunk = total;
-        else return PERFT_ERR_OUT_OF_MEMORY;
-    }
+    // whole level when it fits; otherwise tile-aligned chunks
+    u64 chunk = total <= budgetNodes ? total : (budgetNodes & ~(u64)(TILE_CAP - 1));
+    if (chunk == 0) return PERFT_ERR_OUT_OF_MEMORY;
     if (chunk < total) stats.chunked_levels++;
     for (u64 lo = 0; lo < total; lo += chunk) {
         const u64 hi = std::min(total, lo + chunk);
@@ -628,6 +661,57 @@ int Engine::process_level(const DeviceLevel &L, int remaining, unsigned long lon
         if (rc != PERFT_OK) return rc;
         arenaTop = cm;
     }
+    arenaTop = mark;
+    return PERFT_OK;
+}
+
+// Per-ply slider choice: times every variant on a seeded calibration batch
+// (48 playout positions of 10-30 plies at depth 5) and keeps the fastest for
+// the count-only last ply and, separately, for interior plies.
+int Engine::autotune(bool leaf, bool expand)
+{
+    constexpr u32 N = 48;
+    std::vector<perft_pos48> pos(N);
+    int rc = perft_random_playouts(0xA070707EULL, N, 10, 30, pos.data());
+    if (rc != PERFT_OK) return rc;
+    std::vector<uint8_t> depths(N, 5);
+    const u64 mark = arenaTop;
+    u64 *dPos = (u64 *)alloc(48ull * N);
+    u64 *dOut = (u64 *)alloc(8ull * N);
+    if (!dPos || !dOut) return PERFT_ERR_OUT_OF_MEMORY;
+    ENG_TRY(cudaMemcpyAsync(dPos, pos.data(), 48ull * N, cudaMemcpyHostToDevice, stream));
+    const int keepLeaf = svLeaf, keepExpand = svExpand;
+    auto timed = [&](int l, int e, double &leafMs, double &expandMs) -> int {
+        svLeaf = l;
+        svExpand = e;
+        leafMs = expandMs = 1e30;
+        for (int rep = 0; rep < 3; rep++) {
+            const perft_stats before = stats;
+            const int r = run_batch(dPos, depths.data(), N, dOut);
+            if (r != PERFT_OK) return r;
+            if (rep == 0) continue;  // first run warms caches and clocks
+            leafMs = std::min(leafMs, stats.leaf_ms - before.leaf_ms);
+            expandMs = std::min(expandMs, stats.expand_ms - before.expand_ms);
+        }
+        return PERFT_OK;
+    };
+    int bestLeaf = keepLeaf, bestExpand = keepExpand;
+    double lm, em, best = 1e30;
+    if (leaf) {
+        for (int v = 0; v < SV_COUNT; v++) {
+            if ((rc = timed(v, keepExpand, lm, em)) != PERFT_OK) return rc;
+            if (lm < best) best = lm, bestLeaf = v;
+        }
+    }
+    if (expand) {
+        best = 1e30;
+        for (int v = 0; v < SV_COUNT; v++) {
+            if ((rc = timed(bestLeaf, v, lm, em)) != PERFT_OK) return rc;
+            if (em < best) best = em, bestExpand = v;
+        }
+    }
+    svLeaf = bestLeaf;
+    svExpand = bestExpand;
     arenaTop = mark;
     return PERFT_OK;
 }

@@ -14,8 +14,10 @@ namespace {
 constexpr int NT = 256;
 constexpr int CHAINS = 8;
 
-// kind 0: LOP3 (3-input logic), kind 1: IADD3, kind 2: LOP3/IADD3/SHF mix,
-// kind 3: IMAD (integer multiply-add, the FMA pipe)
+// kind 0: LOP3 (3-input logic), kind 1: integer add, kind 2: LOP3/add/SHF
+// mix, kind 3: IMAD (integer multiply-add, the FMA pipe), kind 4: LOP3 and
+// IMAD alternating (both integer pipes).  Inline PTX keeps the compiler from
+// folding the chains.
 template <int KIND>
 __global__ void __launch_bounds__(NT) k_probe(uint32_t *out, uint32_t seed, int iters)
 {
@@ -25,20 +27,22 @@ __global__ void __launch_bounds__(NT) k_probe(uint32_t *out, uint32_t seed, int 
     for (int it = 0; it < iters; it++) {
 #pragma unroll
         for (int i = 0; i < CHAINS; i++) {
+            uint32_t r = a[i];
             if (KIND == 0) {
-                uint32_t r;
-                asm volatile("lop3.b32 %0, %1, %2, %3, 0x96;" : "=r"(r) : "r"(a[i]), "r"(b), "r"(c));
-                a[i] = r;
+                asm volatile("lop3.b32 %0, %1, %2, %3, 0x96;" : "=r"(r) : "r"(r), "r"(b), "r"(c));
             } else if (KIND == 1) {
-                a[i] = a[i] + b + c;
+                asm volatile("add.u32 %0, %1, %2;" : "=r"(r) : "r"(r), "r"(b));
             } else if (KIND == 2) {
-                uint32_t r;
-                asm volatile("lop3.b32 %0, %1, %2, %3, 0x78;" : "=r"(r) : "r"(a[i]), "r"(b), "r"(c));
-                r = r + b + c;
-                a[i] = __funnelshift_l(r, b, 7);
+                asm volatile("lop3.b32 %0, %1, %2, %3, 0x78;" : "=r"(r) : "r"(r), "r"(b), "r"(c));
+                asm volatile("add.u32 %0, %1, %2;" : "=r"(r) : "r"(r), "r"(c));
+                asm volatile("shf.l.wrap.b32 %0, %1, %2, 7;" : "=r"(r) : "r"(r), "r"(b));
+            } else if (KIND == 3) {
+                asm volatile("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(r), "r"(b), "r"(c));
             } else {
-                a[i] = a[i] * b + c;
+                asm volatile("lop3.b32 %0, %1, %2, %3, 0x96;" : "=r"(r) : "r"(r), "r"(b), "r"(c));
+                asm volatile("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(r), "r"(b), "r"(c));
             }
+            a[i] = r;
         }
     }
     uint32_t s = 0;
@@ -81,16 +85,18 @@ double run(int device, int opsPerChainStep)
 
 extern "C" {
 
-// Writes the measured 32-bit integer operations per second for the four
-// instruction mixes (LOP3, IADD3, LOP3+IADD3+SHF, IMAD).  Returns 0 on success.
-int perft_int32_peak_probe(int device, double out[4])
+// Writes the measured 32-bit integer instructions per second (per lane) for
+// five instruction mixes: LOP3, add, LOP3+add+SHF, IMAD, LOP3+IMAD.
+// Returns 0 on success.
+int perft_int32_peak_probe(int device, double out[5])
 {
     if (cudaSetDevice(device) != cudaSuccess) return -1;
     out[0] = run<0>(device, 1);
-    out[1] = run<1>(device, 1);  // a + b + c is one IADD3 instruction
+    out[1] = run<1>(device, 1);
     out[2] = run<2>(device, 3);
     out[3] = run<3>(device, 1);
-    for (int i = 0; i < 4; i++)
+    out[4] = run<4>(device, 2);
+    for (int i = 0; i < 5; i++)
         if (out[i] <= 0) return -1;
     return 0;
 }

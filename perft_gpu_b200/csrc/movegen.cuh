@@ -72,8 +72,19 @@ enum : u32 {
 
 // Slider attack implementation used by a kernel instantiation.
 enum SliderVariant : int {
-    SV_KOGGE = 0,   // occluded fills, all pieces of a set at once, no tables
-    SV_MAGIC = 1,   // fancy magic lookups, one per piece
+    SV_KOGGE = 0,      // occluded fills, all pieces of a set at once, no tables
+    SV_MAGIC = 1,      // fancy magic lookups, one per piece
+    SV_KOGGE_FMA = 2,  // occluded fills with every constant shift on the FMA pipe
+    SV_KOGGE_MIX = 3,  // FMA-pipe shifts for the opponent's attack map only
+    SV_COUNT = 4,
+};
+
+// Compile-time properties of a variant.
+template <int SV>
+struct SvTraits {
+    static constexpr bool kogge = SV != SV_MAGIC;
+    static constexpr bool fmaAttack = SV == SV_KOGGE_FMA || SV == SV_KOGGE_MIX;
+    static constexpr bool fmaOwn = SV == SV_KOGGE_FMA;
 };
 
 // ------------------------------------------------------------------ tables
@@ -101,6 +112,11 @@ extern u64 h_magic[MAGIC_TABLE_ENTRIES];
 // The one CUDA translation unit (engine.cu) defines the device copies.
 __device__ Tables d_tables;
 __device__ u64 d_magic[MAGIC_TABLE_ENTRIES];
+// c_pow2[k] = 2^k, uploaded at start-up.  Shift amounts read from here are
+// opaque to the compiler, so a multiply by them stays an integer
+// multiply-add on the FMA pipe instead of being folded back into a shift on
+// the (busier) ALU pipe.
+__constant__ u32 c_pow2[32];
 #endif
 
 #ifdef __CUDA_ARCH__
@@ -155,62 +171,121 @@ PG_HD u64 sh_nw(u64 x) { return (x << 7) & ~FILEH; }
 PG_HD u64 sh_se(u64 x) { return (x >> 7) & ~FILEA; }
 PG_HD u64 sh_sw(u64 x) { return (x >> 9) & ~FILEH; }
 
+// ------------------------------------------------- FMA-pipe constant shifts
+// 64-bit shifts by a constant K written as 32x32 multiplies by 2^K, so they
+// issue on the FMA pipe (IMAD.WIDE / IMAD / IMAD.HI) rather than the ALU.
+// Left:  t = lo * 2^K (wide) gives lo << K and lo >> (32-K); hi' = hi*2^K + that.
+// Right: hi * 2^(32-K) (wide) plus umulhi(lo, 2^(32-K)) = lo >> K gives both
+// words at once (the two parts occupy disjoint bits).  Host builds shift.
+template <int K>
+PG_HD u64 shl_fma(u64 x)
+{
+#ifdef __CUDA_ARCH__
+    const u32 lo = (u32)x, hi = (u32)(x >> 32);
+    if (K == 0) return x;
+    if (K >= 32) {
+        if (K == 32) return (u64)lo << 32;
+        return (u64)(lo * c_pow2[K - 32]) << 32;
+    }
+    const u32 m = c_pow2[K];
+    const u64 t = (u64)lo * m;
+    const u32 nhi = hi * m + (u32)(t >> 32);
+    return ((u64)nhi << 32) | (u32)t;
+#else
+    return x << K;
+#endif
+}
+
+template <int K>
+PG_HD u64 shr_fma(u64 x)
+{
+#ifdef __CUDA_ARCH__
+    const u32 lo = (u32)x, hi = (u32)(x >> 32);
+    if (K == 0) return x;
+    if (K >= 32) {
+        if (K == 32) return hi;
+        return __umulhi(hi, c_pow2[64 - K]);
+    }
+    const u32 m = c_pow2[32 - K];
+    return (u64)hi * m + __umulhi(lo, m);
+#else
+    return x >> K;
+#endif
+}
+
+template <int K, bool FMA>
+PG_HD u64 shl(u64 x)
+{
+    if (FMA) return shl_fma<K>(x);
+    return x << K;
+}
+template <int K, bool FMA>
+PG_HD u64 shr(u64 x)
+{
+    if (FMA) return shr_fma<K>(x);
+    return x >> K;
+}
+
 // ------------------------------------------------------------ Kogge-Stone
 // Occluded fill of generator set g through propagator p, then one more step:
 // every square attacked in that direction (first blocker included).  The
 // fill is OR-distributive over generators, and same-direction rays of
 // different pieces never share a non-own square, so per-direction popcounts
 // of a whole piece set sum to the per-piece move counts.
-template <int S, bool LEFT>
+template <int S, bool LEFT, bool FMA>
 PG_HD u64 ks_dir(u64 g, u64 p, u64 wrap)
 {
     p &= wrap;
     if (LEFT) {
-        g |= p & (g << S);
-        p &= p << S;
-        g |= p & (g << (2 * S));
-        p &= p << (2 * S);
-        g |= p & (g << (4 * S));
-        return (g << S) & wrap;
+        g |= p & shl<S, FMA>(g);
+        p &= shl<S, FMA>(p);
+        g |= p & shl<2 * S, FMA>(g);
+        p &= shl<2 * S, FMA>(p);
+        g |= p & shl<4 * S, FMA>(g);
+        return shl<S, FMA>(g) & wrap;
     } else {
-        g |= p & (g >> S);
-        p &= p >> S;
-        g |= p & (g >> (2 * S));
-        p &= p >> (2 * S);
-        g |= p & (g >> (4 * S));
-        return (g >> S) & wrap;
+        g |= p & shr<S, FMA>(g);
+        p &= shr<S, FMA>(p);
+        g |= p & shr<2 * S, FMA>(g);
+        p &= shr<2 * S, FMA>(p);
+        g |= p & shr<4 * S, FMA>(g);
+        return shr<S, FMA>(g) & wrap;
     }
 }
 
-PG_HD u64 ks_north(u64 g, u64 p) { return ks_dir<8, true>(g, p, ~0ULL); }
-PG_HD u64 ks_south(u64 g, u64 p) { return ks_dir<8, false>(g, p, ~0ULL); }
-PG_HD u64 ks_east(u64 g, u64 p) { return ks_dir<1, true>(g, p, ~FILEA); }
-PG_HD u64 ks_west(u64 g, u64 p) { return ks_dir<1, false>(g, p, ~FILEH); }
-PG_HD u64 ks_ne(u64 g, u64 p) { return ks_dir<9, true>(g, p, ~FILEA); }
-PG_HD u64 ks_nw(u64 g, u64 p) { return ks_dir<7, true>(g, p, ~FILEH); }
-PG_HD u64 ks_se(u64 g, u64 p) { return ks_dir<7, false>(g, p, ~FILEA); }
-PG_HD u64 ks_sw(u64 g, u64 p) { return ks_dir<9, false>(g, p, ~FILEH); }
+template <bool F = false> PG_HD u64 ks_north(u64 g, u64 p) { return ks_dir<8, true, F>(g, p, ~0ULL); }
+template <bool F = false> PG_HD u64 ks_south(u64 g, u64 p) { return ks_dir<8, false, F>(g, p, ~0ULL); }
+template <bool F = false> PG_HD u64 ks_east(u64 g, u64 p) { return ks_dir<1, true, F>(g, p, ~FILEA); }
+template <bool F = false> PG_HD u64 ks_west(u64 g, u64 p) { return ks_dir<1, false, F>(g, p, ~FILEH); }
+template <bool F = false> PG_HD u64 ks_ne(u64 g, u64 p) { return ks_dir<9, true, F>(g, p, ~FILEA); }
+template <bool F = false> PG_HD u64 ks_nw(u64 g, u64 p) { return ks_dir<7, true, F>(g, p, ~FILEH); }
+template <bool F = false> PG_HD u64 ks_se(u64 g, u64 p) { return ks_dir<7, false, F>(g, p, ~FILEA); }
+template <bool F = false> PG_HD u64 ks_sw(u64 g, u64 p) { return ks_dir<9, false, F>(g, p, ~FILEH); }
 
+template <bool F = false>
 PG_HD u64 ks_diag(u64 g, u64 empty)
 {
-    return ks_ne(g, empty) | ks_nw(g, empty) | ks_se(g, empty) | ks_sw(g, empty);
+    return ks_ne<F>(g, empty) | ks_nw<F>(g, empty) | ks_se<F>(g, empty) | ks_sw<F>(g, empty);
 }
+template <bool F = false>
 PG_HD u64 ks_orth(u64 g, u64 empty)
 {
-    return ks_north(g, empty) | ks_south(g, empty) | ks_east(g, empty) | ks_west(g, empty);
+    return ks_north<F>(g, empty) | ks_south<F>(g, empty) | ks_east<F>(g, empty) | ks_west<F>(g, empty);
 }
 
 // Per-direction move counts of a whole slider set (targets = squares the
 // pieces may land on).
+template <bool F = false>
 PG_HD int ks_count_diag(u64 g, u64 empty, u64 targets)
 {
-    return popc(ks_ne(g, empty) & targets) + popc(ks_nw(g, empty) & targets) +
-           popc(ks_se(g, empty) & targets) + popc(ks_sw(g, empty) & targets);
+    return popc(ks_ne<F>(g, empty) & targets) + popc(ks_nw<F>(g, empty) & targets) +
+           popc(ks_se<F>(g, empty) & targets) + popc(ks_sw<F>(g, empty) & targets);
 }
+template <bool F = false>
 PG_HD int ks_count_orth(u64 g, u64 empty, u64 targets)
 {
-    return popc(ks_north(g, empty) & targets) + popc(ks_south(g, empty) & targets) +
-           popc(ks_east(g, empty) & targets) + popc(ks_west(g, empty) & targets);
+    return popc(ks_north<F>(g, empty) & targets) + popc(ks_south<F>(g, empty) & targets) +
+           popc(ks_east<F>(g, empty) & targets) + popc(ks_west<F>(g, empty) & targets);
 }
 
 // ------------------------------------------------------------------ magics
@@ -230,20 +305,20 @@ template <int SV>
 PG_HD u64 bishop_att(int sq, u64 occ)
 {
     if (SV == SV_MAGIC) return magic_bishop(sq, occ);
-    return ks_diag(1ULL << sq, ~occ);
+    return ks_diag<SvTraits<SV>::fmaOwn>(1ULL << sq, ~occ);
 }
 template <int SV>
 PG_HD u64 rook_att(int sq, u64 occ)
 {
     if (SV == SV_MAGIC) return magic_rook(sq, occ);
-    return ks_orth(1ULL << sq, ~occ);
+    return ks_orth<SvTraits<SV>::fmaOwn>(1ULL << sq, ~occ);
 }
 
 // Union of the attacks of a slider set; occ excludes transparent squares.
 template <int SV>
 PG_HD u64 bishop_set_att(u64 set, u64 occ)
 {
-    if (SV == SV_KOGGE) return ks_diag(set, ~occ);
+    if (SvTraits<SV>::kogge) return ks_diag<SvTraits<SV>::fmaAttack>(set, ~occ);
     u64 a = 0;
     while (set) {
         a |= magic_bishop(ctz(set), occ);
@@ -254,7 +329,7 @@ PG_HD u64 bishop_set_att(u64 set, u64 occ)
 template <int SV>
 PG_HD u64 rook_set_att(u64 set, u64 occ)
 {
-    if (SV == SV_KOGGE) return ks_orth(set, ~occ);
+    if (SvTraits<SV>::kogge) return ks_orth<SvTraits<SV>::fmaAttack>(set, ~occ);
     u64 a = 0;
     while (set) {
         a |= magic_rook(ctz(set), occ);
@@ -318,14 +393,6 @@ PG_HD void setup_ctx(const Board &b, Ctx &c)
                  bishop_set_att<SV>(c.tB, occNoK) | rook_set_att<SV>(c.tR, occNoK);
 }
 
-// Checkers of the side to move's king.
-template <int SV>
-PG_HD u64 checkers_of(const Board &b, const Ctx &c)
-{
-    return (pawn_att_up(c.myK) & c.tP) | (PG_TAB(knight[c.ksq]) & c.tN) |
-           (bishop_att<SV>(c.ksq, c.occ) & c.tB) | (rook_att<SV>(c.ksq, c.occ) & c.tR);
-}
-
 // Pinned pieces of the side to move (findPinnedPieces, MoveGeneratorBitboard.h:1213-1249).
 PG_HD u64 pinned_of(const Ctx &c)
 {
@@ -351,48 +418,22 @@ PG_HD bool ep_exposes_king(const Ctx &c, u64 src, u64 captured)
 }
 
 // ------------------------------------------------------------------- count
-// Legal move count when in check (countMovesOutOfCheck).
+// Check mask of the side to move: every square when not in check; the
+// checker plus the squares between it and the king in single check; nothing
+// in double check.  Non-king moves must land inside it.  A pinned piece can
+// never resolve a check (its pin line meets the check line only at the
+// king), so pinned moves are dropped in check.  This folds the reference's
+// separate out-of-check routines (countMovesOutOfCheck /
+// generateMovesOutOfCheck) into the main path, so a warp with one lane in
+// check does not run a second move generator for it.
 template <int SV>
-PG_HD u32 count_evasions(const Board &b, const Ctx &c)
+PG_HD u64 check_mask(const Ctx &c)
 {
-    const u64 notMine = ~c.mine;
-    u32 n = popc(PG_TAB(king[c.ksq]) & notMine & ~c.attacked);
-    const u64 chk = checkers_of<SV>(b, c);
-    if (chk & (chk - 1)) return n;  // double check: king moves only
-    const int csq = ctz(chk);
-    const u64 safe = chk | PG_TAB(between[c.ksq][csq]);
-    const u64 pinned = pinned_of(c);
-    const u64 free = c.mine & ~pinned;
-
-    const u64 P = c.pawns & free;
-    const u64 p1 = sh_n(P) & c.empty;
-    const u64 p1s = p1 & safe;
-    n += popc(p1s) + 3 * popc(p1s & RANK8);
-    n += popc(sh_n(p1 & RANK3) & c.empty & safe);
-    const u64 cl = sh_nw(P) & chk, cr = sh_ne(P) & chk;
-    n += popc(cl) + popc(cr) + 3 * (popc(cl & RANK8) + popc(cr & RANK8));
-    const u32 epf = c.st >> 4;
-    if (epf) {
-        const u64 target = 1ULL << (39 + epf);
-        if (sh_s(target) == chk) n += popc(pawn_att_down(target) & P);
-    }
-
-    u64 N = b.knights & free;
-    while (N) {
-        n += popc(PG_TAB(knight[ctz(N)]) & safe);
-        N &= N - 1;
-    }
-    u64 B = b.bq & free;
-    while (B) {
-        n += popc(bishop_att<SV>(ctz(B), c.occ) & safe);
-        B &= B - 1;
-    }
-    u64 R = b.rq & free;
-    while (R) {
-        n += popc(rook_att<SV>(ctz(R), c.occ) & safe);
-        R &= R - 1;
-    }
-    return n;
+    if (!(c.attacked & c.myK)) return ~0ULL;
+    const u64 chk = (pawn_att_up(c.myK) & c.tP) | (PG_TAB(knight[c.ksq]) & c.tN) |
+                    (magic_bishop(c.ksq, c.occ) & c.tB) | (magic_rook(c.ksq, c.occ) & c.tR);
+    if (chk & (chk - 1)) return 0;
+    return chk | PG_TAB(between[c.ksq][ctz(chk)]);
 }
 
 // Legal move count of the side to move (countMoves).
@@ -401,14 +442,18 @@ PG_HD u32 count_moves(const Board &b)
 {
     Ctx c;
     setup_ctx<SV>(b, c);
-    if (c.attacked & c.myK) return count_evasions<SV>(b, c);
-
     const u64 notMine = ~c.mine;
     u32 n = popc(PG_TAB(king[c.ksq]) & notMine & ~c.attacked);
+    const u64 cm = check_mask<SV>(c);
+    if (!cm) return n;  // double check: king moves only
+    const bool inCheck = cm != ~0ULL;
+    const u64 targets = notMine & cm;
 
-    // castling (relative squares: king e1, rooks h1/a1)
-    if ((c.st & 1) && !((c.occ | c.attacked) & 0x60ULL)) n++;
-    if ((c.st & 2) && !(c.occ & 0x0EULL) && !(c.attacked & 0x0CULL)) n++;
+    // castling (relative squares: king e1, rooks h1/a1), never out of check
+    if (!inCheck) {
+        if ((c.st & 1) && !((c.occ | c.attacked) & 0x60ULL)) n++;
+        if ((c.st & 2) && !(c.occ & 0x0EULL) && !(c.attacked & 0x0CULL)) n++;
+    }
 
     // pins: each pinned piece may only move along its pin line
     u64 pinned = 0;
@@ -420,6 +465,7 @@ PG_HD u32 count_moves(const Board &b)
         const u64 blk = btw & c.occ;
         if (!blk || (blk & (blk - 1)) || !(blk & c.mine)) continue;
         pinned |= blk;
+        if (inCheck) continue;
         const bool diag = (PG_TAB(bishopRays[c.ksq]) >> s) & 1;
         if (blk & (diag ? b.bq : b.rq)) {
             n += popc(btw);  // every square between king and pinner, minus its own, plus the capture
@@ -437,36 +483,40 @@ PG_HD u32 count_moves(const Board &b)
     // free pawns, set-wise
     const u64 P = c.pawns & c.mine & ~pinned;
     const u64 p1 = sh_n(P) & c.empty;
-    n += popc(p1) + 3 * popc(p1 & RANK8);
-    n += popc(sh_n(p1 & RANK3) & c.empty);
-    const u64 cl = sh_nw(P) & c.theirs, cr = sh_ne(P) & c.theirs;
+    const u64 p1c = p1 & cm;
+    n += popc(p1c) + 3 * popc(p1c & RANK8);
+    n += popc(sh_n(p1 & RANK3) & c.empty & cm);
+    const u64 capT = c.theirs & cm;
+    const u64 cl = sh_nw(P) & capT, cr = sh_ne(P) & capT;
     n += popc(cl) + popc(cr) + 3 * (popc(cl & RANK8) + popc(cr & RANK8));
 
-    // en passant
+    // en passant: out of check, or capturing the checking pawn
     const u32 epf = c.st >> 4;
     if (epf) {
         const u64 target = 1ULL << (39 + epf);
         const u64 captured = sh_s(target);
-        u64 srcs = pawn_att_down(target) & c.pawns & c.mine;
-        while (srcs) {
-            const u64 s = srcs & (0 - srcs);
-            srcs ^= s;
-            if (s & pinned) {
-                if (PG_TAB(line[ctz(s)][c.ksq]) & target) n++;
-            } else if (!ep_exposes_king(c, s, captured)) {
-                n++;
+        if (!inCheck || (captured & cm)) {
+            u64 srcs = pawn_att_down(target) & c.pawns & c.mine;
+            while (srcs) {
+                const u64 s = srcs & (0 - srcs);
+                srcs ^= s;
+                if (s & pinned) {
+                    if (!inCheck && (PG_TAB(line[ctz(s)][c.ksq]) & target)) n++;
+                } else if (!ep_exposes_king(c, s, captured)) {
+                    n++;
+                }
             }
         }
     }
 
     // knights
     const u64 N = b.knights & c.mine & ~pinned;
-    if (SV == SV_KOGGE) {
-        n += knight_set_count(N, notMine);
+    if (SvTraits<SV>::kogge) {
+        n += knight_set_count(N, targets);
     } else {
         u64 k = N;
         while (k) {
-            n += popc(PG_TAB(knight[ctz(k)]) & notMine);
+            n += popc(PG_TAB(knight[ctz(k)]) & targets);
             k &= k - 1;
         }
     }
@@ -474,17 +524,18 @@ PG_HD u32 count_moves(const Board &b)
     // sliders
     const u64 B = b.bq & c.mine & ~pinned;
     const u64 R = b.rq & c.mine & ~pinned;
-    if (SV == SV_KOGGE) {
-        n += ks_count_diag(B, c.empty, notMine) + ks_count_orth(R, c.empty, notMine);
+    if (SvTraits<SV>::kogge) {
+        constexpr bool F = SvTraits<SV>::fmaOwn;
+        n += ks_count_diag<F>(B, c.empty, targets) + ks_count_orth<F>(R, c.empty, targets);
     } else {
         u64 x = B;
         while (x) {
-            n += popc(magic_bishop(ctz(x), c.occ) & notMine);
+            n += popc(magic_bishop(ctz(x), c.occ) & targets);
             x &= x - 1;
         }
         x = R;
         while (x) {
-            n += popc(magic_rook(ctz(x), c.occ) & notMine);
+            n += popc(magic_rook(ctz(x), c.occ) & targets);
             x &= x - 1;
         }
     }
@@ -530,56 +581,20 @@ PG_HD void gen_moves(const Board &b, Sink &out)
     setup_ctx<SV>(b, c);
     const u64 notMine = ~c.mine;
     emit_targets(out, c.ksq, PG_TAB(king[c.ksq]) & notMine & ~c.attacked);
+    const u64 cm = check_mask<SV>(c);
+    if (!cm) return;
+    const bool inCheck = cm != ~0ULL;
+    const u64 targets = notMine & cm;
 
-    if (c.attacked & c.myK) {
-        const u64 chk = checkers_of<SV>(b, c);
-        if (chk & (chk - 1)) return;
-        const u64 safe = chk | PG_TAB(between[c.ksq][ctz(chk)]);
-        const u64 free = c.mine & ~pinned_of(c);
-        u64 P = c.pawns & free;
-        const u32 epf = c.st >> 4;
-        const u64 epTarget = epf ? (1ULL << (39 + epf)) : 0;
-        const bool epSaves = epf && sh_s(epTarget) == chk;
-        while (P) {
-            const int from = ctz(P);
-            const u64 p = P & (0 - P);
-            P ^= p;
-            const u64 p1 = sh_n(p) & c.empty;
-            if (p1 & safe) emit_pawn(out, from, from + 8, MF_QUIET);
-            const u64 p2 = sh_n(p1 & RANK3) & c.empty & safe;
-            if (p2) out(encode_move(from, from + 16, MF_DOUBLE_PUSH));
-            const u64 cap = pawn_att_up(p) & chk;
-            if (cap) emit_pawn(out, from, ctz(cap), MF_CAPTURE);
-            if (epSaves && (pawn_att_up(p) & epTarget)) out(encode_move(from, ctz(epTarget), MF_EP));
-        }
-        u64 N = b.knights & free;
-        while (N) {
-            const int s = ctz(N);
-            N &= N - 1;
-            emit_targets(out, s, PG_TAB(knight[s]) & safe);
-        }
-        u64 B = b.bq & free;
-        while (B) {
-            const int s = ctz(B);
-            B &= B - 1;
-            emit_targets(out, s, bishop_att<SV>(s, c.occ) & safe);
-        }
-        u64 R = b.rq & free;
-        while (R) {
-            const int s = ctz(R);
-            R &= R - 1;
-            emit_targets(out, s, rook_att<SV>(s, c.occ) & safe);
-        }
-        return;
+    if (!inCheck) {
+        if ((c.st & 1) && !((c.occ | c.attacked) & 0x60ULL)) out(encode_move(4, 6, MF_KING_CASTLE));
+        if ((c.st & 2) && !(c.occ & 0x0EULL) && !(c.attacked & 0x0CULL)) out(encode_move(4, 2, MF_QUEEN_CASTLE));
     }
-
-    if ((c.st & 1) && !((c.occ | c.attacked) & 0x60ULL)) out(encode_move(4, 6, MF_KING_CASTLE));
-    if ((c.st & 2) && !(c.occ & 0x0EULL) && !(c.attacked & 0x0CULL)) out(encode_move(4, 2, MF_QUEEN_CASTLE));
 
     const u64 pinned = pinned_of(c);
 
-    // pinned pieces: along the pin line only
-    u64 pp = pinned;
+    // pinned pieces: along the pin line only, never in check
+    u64 pp = inCheck ? 0 : pinned;
     while (pp) {
         const int s = ctz(pp);
         const u64 p = pp & (0 - pp);
@@ -607,26 +622,27 @@ PG_HD void gen_moves(const Board &b, Sink &out)
     while (N) {
         const int s = ctz(N);
         N &= N - 1;
-        emit_targets(out, s, PG_TAB(knight[s]) & notMine);
+        emit_targets(out, s, PG_TAB(knight[s]) & targets);
     }
     u64 B = b.bq & c.mine & ~pinned;
     while (B) {
         const int s = ctz(B);
         B &= B - 1;
-        emit_targets(out, s, bishop_att<SV>(s, c.occ) & notMine);
+        emit_targets(out, s, bishop_att<SV>(s, c.occ) & targets);
     }
     u64 R = b.rq & c.mine & ~pinned;
     while (R) {
         const int s = ctz(R);
         R &= R - 1;
-        emit_targets(out, s, rook_att<SV>(s, c.occ) & notMine);
+        emit_targets(out, s, rook_att<SV>(s, c.occ) & targets);
     }
     const u64 P = c.pawns & c.mine & ~pinned;
-    u64 p1 = sh_n(P) & c.empty;
-    u64 p2 = sh_n(p1 & RANK3) & c.empty;
-    while (p1) {
-        const int to = ctz(p1);
-        p1 &= p1 - 1;
+    const u64 p1 = sh_n(P) & c.empty;
+    u64 p1c = p1 & cm;
+    u64 p2 = sh_n(p1 & RANK3) & c.empty & cm;
+    while (p1c) {
+        const int to = ctz(p1c);
+        p1c &= p1c - 1;
         emit_pawn(out, to - 8, to, MF_QUIET);
     }
     while (p2) {
@@ -634,13 +650,14 @@ PG_HD void gen_moves(const Board &b, Sink &out)
         p2 &= p2 - 1;
         out(encode_move(to - 16, to, MF_DOUBLE_PUSH));
     }
-    u64 cl = sh_nw(P) & c.theirs;
+    const u64 capT = c.theirs & cm;
+    u64 cl = sh_nw(P) & capT;
     while (cl) {
         const int to = ctz(cl);
         cl &= cl - 1;
         emit_pawn(out, to - 7, to, MF_CAPTURE);
     }
-    u64 cr = sh_ne(P) & c.theirs;
+    u64 cr = sh_ne(P) & capT;
     while (cr) {
         const int to = ctz(cr);
         cr &= cr - 1;
@@ -650,13 +667,15 @@ PG_HD void gen_moves(const Board &b, Sink &out)
     if (epf) {
         const u64 target = 1ULL << (39 + epf);
         const u64 captured = sh_s(target);
-        u64 srcs = pawn_att_down(target) & c.pawns & c.mine;
-        while (srcs) {
-            const u64 s = srcs & (0 - srcs);
-            srcs ^= s;
-            bool ok = (s & pinned) ? ((PG_TAB(line[ctz(s)][c.ksq]) & target) != 0)
-                                   : !ep_exposes_king(c, s, captured);
-            if (ok) out(encode_move(ctz(s), 39 + epf, MF_EP));
+        if (!inCheck || (captured & cm)) {
+            u64 srcs = pawn_att_down(target) & c.pawns & c.mine;
+            while (srcs) {
+                const u64 s = srcs & (0 - srcs);
+                srcs ^= s;
+                const bool ok = (s & pinned) ? (!inCheck && (PG_TAB(line[ctz(s)][c.ksq]) & target) != 0)
+                                             : !ep_exposes_king(c, s, captured);
+                if (ok) out(encode_move(ctz(s), 39 + epf, MF_EP));
+            }
         }
     }
 }

@@ -124,16 +124,28 @@ def test_divide_sums_to_perft(engine):
         assert sorted(div) == sorted(engine.legal_moves(p))
 
 
-def test_magic_sliders_variant(engine, golden):
-    engine.init(device=0, arena_bytes=2 << 30, sliders_expand=engine.SLIDERS_MAGIC,
-                sliders_leaf=engine.SLIDERS_MAGIC)
+@pytest.mark.parametrize("variant", [0, 1, 2, 3], ids=["kogge", "magic", "kogge_fma", "kogge_mix"])
+def test_slider_variants(engine, golden, oracle, variant):
+    """Every slider variant, on interior and last plies alike, is bit-exact."""
+    engine.init(device=0, arena_bytes=2 << 30, sliders_expand=variant, sliders_leaf=variant)
     try:
         st = engine.stats()
-        assert st["sliders_leaf"] == engine.SLIDERS_MAGIC
-        for name, pos, d, c in _golden_items(golden, max_leaves=20_000_000):
-            assert engine.perft(pos, d) == c, (name, d)
+        assert st["sliders_leaf"] == variant and st["sliders_expand"] == variant
+        items = list(_golden_items(golden, max_leaves=20_000_000))
+        pos = np.stack([p for _, p, _, _ in items])
+        depths = np.array([d for _, _, d, _ in items], dtype=np.uint8)
+        want = np.array([c for _, _, _, c in items], dtype=np.uint64)
+        assert np.array_equal(engine.perft_batch(pos, depths), want)
+        rnd = engine.random_playouts(seed=600 + variant, n=256, min_plies=0, max_plies=80)
+        d = (np.arange(256) % 4 + 1).astype(np.uint8)
+        assert np.array_equal(engine.perft_batch(rnd, d), oracle.perft_batch_mt(rnd, d))
     finally:
         engine.init(device=0, arena_bytes=8 << 30)
+
+
+def test_autotuner_choice_is_reported(engine):
+    st = engine.stats()
+    assert st["sliders_leaf"] in engine.SLIDER_NAMES and st["sliders_expand"] in engine.SLIDER_NAMES
 
 
 def test_small_arena_chunks_levels(engine, golden):

@@ -1,0 +1,70 @@
+"""The product's move generator (movegen.cuh), compiled for the host, against
+the oracle: legal-move counts, generated children and perft, for both slider
+variants.  Runs without a GPU."""
+import ctypes
+import os
+import random
+import subprocess
+
+import numpy as np
+import pytest
+
+from tests._oracle import P6, ROOT, pos48_from_hex
+
+HC_DIR = os.path.join(ROOT, "tests", "hostcheck")
+HC_LIB = os.path.join(HC_DIR, "libhostcheck.so")
+
+
+@pytest.fixture(scope="module")
+def hc():
+    src = [os.path.join(HC_DIR, "hostcheck.cpp"), os.path.join(ROOT, "perft_gpu_b200", "csrc", "tables.cpp")]
+    hdr = os.path.join(ROOT, "perft_gpu_b200", "csrc", "movegen.cuh")
+    if not os.path.exists(HC_LIB) or any(os.path.getmtime(s) > os.path.getmtime(HC_LIB) for s in src + [hdr]):
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", HC_LIB] + src, check=True)
+    lib = ctypes.CDLL(HC_LIB)
+    lib.hc_count.restype = ctypes.c_uint32
+    lib.hc_children.restype = ctypes.c_uint32
+    lib.hc_perft.restype = ctypes.c_uint64
+    lib.hc_init()
+    return lib
+
+
+def _children(hc, pos, sv):
+    buf = (ctypes.c_uint64 * (6 * 256))()
+    n = hc.hc_children(P6(*[int(x) for x in pos]), sv, buf)
+    return sorted(tuple(buf[6 * i:6 * i + 6]) for i in range(n))
+
+
+@pytest.mark.parametrize("sv", [0, 1], ids=["kogge", "magic"])
+def test_golden_perft(hc, golden, sv):
+    for e in golden:
+        p = P6(*[int(h, 16) for h in e["pos48"]])
+        for d, c in e["counts"].items():
+            if int(c) <= 3_000_000:
+                assert hc.hc_perft(p, int(d), sv) == int(c), (e["name"], d)
+
+
+@pytest.mark.parametrize("sv", [0, 1], ids=["kogge", "magic"])
+def test_counts_and_children_vs_oracle(hc, oracle, sv):
+    rng = random.Random(3 + sv)
+    start = oracle.fen_to_pos("rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1")
+    positions = 0
+    for _ in range(120):
+        p = start
+        for _ in range(rng.randint(0, 80)):
+            kids = oracle.children(p)
+            assert hc.hc_count(P6(*[int(x) for x in p]), sv) == len(kids)
+            assert _children(hc, p, sv) == sorted(tuple(int(x) for x in k) for k in kids)
+            positions += 1
+            if not kids:
+                break
+            p = kids[rng.randrange(len(kids))]
+    assert positions > 2000
+
+
+def test_relative_roundtrip(hc, golden):
+    out = P6()
+    for e in golden:
+        p = P6(*[int(h, 16) for h in e["pos48"]])
+        hc.hc_roundtrip(p, out)
+        assert list(out) == list(p), e["name"]
