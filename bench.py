@@ -108,10 +108,11 @@ def load_work_figures():
 def int32_peak(device):
     """Measured integer-pipe peak (ops/s) from libperft_probe.so."""
     lib = ctypes.CDLL(os.path.join(ROOT, "perft_gpu_b200", "libperft_probe.so"))
-    out = (ctypes.c_double * 5)()
+    out = (ctypes.c_double * 7)()
     if lib.perft_int32_peak_probe(device, out) != 0:
         return None
-    return {"lop3": out[0], "iadd": out[1], "lop3_iadd_shf": out[2], "imad": out[3], "lop3_imad": out[4]}
+    return {"lop3": out[0], "iadd": out[1], "lop3_iadd_shf": out[2], "imad": out[3], "lop3_imad": out[4],
+            "imad_hi": out[5], "imad_wide_lop3": out[6]}
 
 
 def traffic_from_profiles(workload):
@@ -356,7 +357,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["batch", "start", "deep"], default="batch")
-    ap.add_argument("--sliders", choices=["auto", "kogge", "magic", "kogge_fma", "kogge_mix"], default="auto")
+    ap.add_argument("--sliders", choices=["auto", "kogge", "magic", "kogge_fma", "kogge_split"], default="auto")
     ap.add_argument("--positions", type=int, default=4096,
                     help="batch workload: use the first N positions (profiling runs)")
     ap.add_argument("--arena-gb", type=float, default=0.0, help="level-buffer arena (0 = 85%% of free HBM)")

@@ -56,7 +56,7 @@ typedef struct perft_pos48 {
 #define PERFT_SLIDERS_KOGGE      0  /* Kogge-Stone occluded fills */
 #define PERFT_SLIDERS_MAGIC      1  /* fancy magic lookups */
 #define PERFT_SLIDERS_KOGGE_FMA  2  /* Kogge-Stone, constant shifts on the FMA pipe */
-#define PERFT_SLIDERS_KOGGE_MIX  3  /* Kogge-Stone, FMA-pipe shifts for attack maps only */
+#define PERFT_SLIDERS_KOGGE_SPLIT 3 /* Kogge-Stone, left shifts split over ALU and FMA pipes */
 
 typedef struct perft_config {
     int      device;          /* CUDA device ordinal */

@@ -19,7 +19,8 @@ from typing import Iterable, List, Sequence
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libperft_b200.so")
+# PERFT_B200_LIB points the binding at another build of the same library
+LIB_PATH = os.environ.get("PERFT_B200_LIB") or os.path.join(_HERE, "libperft_b200.so")
 
 PERFT_OK = 0
 PERFT_ERR_INVALID_ARG = -1
@@ -37,9 +38,9 @@ SLIDERS_AUTO = -1
 SLIDERS_KOGGE = 0
 SLIDERS_MAGIC = 1
 SLIDERS_KOGGE_FMA = 2
-SLIDERS_KOGGE_MIX = 3
+SLIDERS_KOGGE_SPLIT = 3
 SLIDER_NAMES = {SLIDERS_KOGGE: "kogge", SLIDERS_MAGIC: "magic", SLIDERS_KOGGE_FMA: "kogge_fma",
-                SLIDERS_KOGGE_MIX: "kogge_mix"}
+                SLIDERS_KOGGE_SPLIT: "kogge_split"}
 
 START_FEN = "rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1"
 

@@ -36,12 +36,18 @@ def up_to_date(lib, sources):
     return all(os.path.getmtime(d) <= t for d in deps)
 
 
-def _nvcc(lib, sources, verbose):
-    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + [
+def _nvcc(lib, sources, verbose, defines=()):
+    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + [f"-D{d}" for d in defines] + [
         "-I", os.path.join(ROOT, "include"),
         "-o", lib,
     ] + [os.path.join(CSRC, s) for s in sources] + ["-lcudart"]
     subprocess.run(cmd, check=True)
+
+
+def build_variant(out, defines, verbose=False):
+    """Compiles the engine with extra -D definitions into `out` (tuning builds)."""
+    _nvcc(out, SOURCES, verbose, defines)
+    return out
 
 
 def build(verbose=False, force=False):

@@ -38,6 +38,7 @@
 #include <vector>
 
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "../../include/perft_b200.h"
@@ -52,10 +53,17 @@ using namespace pg;
 namespace {
 
 // ------------------------------------------------------------- constants
+#ifndef PG_TILE_CAP_LOG2
+#define PG_TILE_CAP_LOG2 13
+#endif
+#ifndef PG_TILE_MINB
+#define PG_TILE_MINB 3
+#endif
 constexpr int TILE_NT = 256;
-constexpr int TILE_CAP_LOG2 = 12;
+constexpr int TILE_CAP_LOG2 = PG_TILE_CAP_LOG2;  // items per tile = 2^TILE_CAP_LOG2
 constexpr int TILE_CAP = 1 << TILE_CAP_LOG2;
 constexpr int TILE_MAXP = TILE_NT;
+constexpr int TILE_MINB = PG_TILE_MINB;          // resident CTAs per SM the register budget targets
 constexpr int MAX_LEGAL_MOVES = 218;
 
 constexpr int SCAN_NT = 512;
@@ -254,14 +262,14 @@ struct WindowSink {
 };
 
 template <int MODE, int SV>
-__global__ void __launch_bounds__(TILE_NT, 2) k_tile(const TileParams P)
+__global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams P)
 {
     __shared__ u64 sb[6][TILE_MAXP];
     __shared__ u32 sroot[TILE_MAXP];
     __shared__ u32 srun[TILE_MAXP];
     __shared__ u32 srunRoot[TILE_MAXP];
     __shared__ unsigned long long sacc[TILE_MAXP];
-    __shared__ u32 sitems[TILE_CAP];
+    extern __shared__ __align__(16) u32 sitems[];  // TILE_CAP items (dynamic: may exceed 48 KB)
     __shared__ int swarp[TILE_NT / 32];
     __shared__ u32 sTile;
 
@@ -398,6 +406,7 @@ private:
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int svExpand = SV_KOGGE, svLeaf = SV_KOGGE;
     int gridTile[2][SV_COUNT] = {};
+    bool trace = false;  // PERFT_TRACE=1: one stderr line per tile launch
 
     void *alloc(u64 bytes)
     {
@@ -433,11 +442,17 @@ int Engine::check(cudaError_t e, const char *what)
         if (rc_ != PERFT_OK) return rc_;                \
     } while (0)
 
+constexpr size_t TILE_DYN_SMEM = sizeof(u32) * TILE_CAP;
+
+// Allows the item list's dynamic shared memory on one instantiation and
+// returns its resident-CTA grid (SMs x CTAs per SM).
 template <int MODE, int SV>
 int occupancy_grid(int nsm)
 {
+    cudaFuncSetAttribute(k_tile<MODE, SV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_DYN_SMEM);
     int perSm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_tile<MODE, SV>, TILE_NT, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_tile<MODE, SV>, TILE_NT, TILE_DYN_SMEM) !=
+            cudaSuccess ||
         perSm < 1)
         perSm = 1;
     return perSm * nsm;
@@ -447,10 +462,10 @@ template <int MODE>
 void launch_tile_variant(int sv, int grid, cudaStream_t st, const TileParams &P)
 {
     switch (sv) {
-    case SV_MAGIC: k_tile<MODE, SV_MAGIC><<<grid, TILE_NT, 0, st>>>(P); break;
-    case SV_KOGGE_FMA: k_tile<MODE, SV_KOGGE_FMA><<<grid, TILE_NT, 0, st>>>(P); break;
-    case SV_KOGGE_MIX: k_tile<MODE, SV_KOGGE_MIX><<<grid, TILE_NT, 0, st>>>(P); break;
-    default: k_tile<MODE, SV_KOGGE><<<grid, TILE_NT, 0, st>>>(P); break;
+    case SV_MAGIC: k_tile<MODE, SV_MAGIC><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P); break;
+    case SV_KOGGE_FMA: k_tile<MODE, SV_KOGGE_FMA><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P); break;
+    case SV_KOGGE_SPLIT: k_tile<MODE, SV_KOGGE_SPLIT><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P); break;
+    default: k_tile<MODE, SV_KOGGE><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P); break;
     }
 }
 
@@ -460,7 +475,7 @@ const char *slider_name(int sv)
     case SV_KOGGE: return "kogge";
     case SV_MAGIC: return "magic";
     case SV_KOGGE_FMA: return "kogge_fma";
-    case SV_KOGGE_MIX: return "kogge_mix";
+    case SV_KOGGE_SPLIT: return "kogge_split";
     default: return "?";
     }
 }
@@ -471,6 +486,7 @@ int Engine::init(const perft_config &cfg)
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return PERFT_ERR_NO_DEVICE;
     if (cfg.device < 0 || cfg.device >= ndev) return PERFT_ERR_INVALID_ARG;
     device = cfg.device;
+    trace = getenv("PERFT_TRACE") && getenv("PERFT_TRACE")[0] == '1';
     ENG_TRY(cudaSetDevice(device));
     cudaDeviceProp prop;
     ENG_TRY(cudaGetDeviceProperties(&prop, device));
@@ -502,11 +518,11 @@ int Engine::init(const perft_config &cfg)
     gridTile[MODE_EXPAND][SV_KOGGE] = occupancy_grid<MODE_EXPAND, SV_KOGGE>(nsm);
     gridTile[MODE_EXPAND][SV_MAGIC] = occupancy_grid<MODE_EXPAND, SV_MAGIC>(nsm);
     gridTile[MODE_EXPAND][SV_KOGGE_FMA] = occupancy_grid<MODE_EXPAND, SV_KOGGE_FMA>(nsm);
-    gridTile[MODE_EXPAND][SV_KOGGE_MIX] = occupancy_grid<MODE_EXPAND, SV_KOGGE_MIX>(nsm);
+    gridTile[MODE_EXPAND][SV_KOGGE_SPLIT] = occupancy_grid<MODE_EXPAND, SV_KOGGE_SPLIT>(nsm);
     gridTile[MODE_LEAF][SV_KOGGE] = occupancy_grid<MODE_LEAF, SV_KOGGE>(nsm);
     gridTile[MODE_LEAF][SV_MAGIC] = occupancy_grid<MODE_LEAF, SV_MAGIC>(nsm);
     gridTile[MODE_LEAF][SV_KOGGE_FMA] = occupancy_grid<MODE_LEAF, SV_KOGGE_FMA>(nsm);
-    gridTile[MODE_LEAF][SV_KOGGE_MIX] = occupancy_grid<MODE_LEAF, SV_KOGGE_MIX>(nsm);
+    gridTile[MODE_LEAF][SV_KOGGE_SPLIT] = occupancy_grid<MODE_LEAF, SV_KOGGE_SPLIT>(nsm);
 
     auto pick = [](int v) { return (v >= 0 && v < SV_COUNT) ? v : SV_KOGGE; };
     svExpand = pick(cfg.sliders_expand);
@@ -609,6 +625,10 @@ int Engine::launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, 
     ENG_TRY(cudaEventSynchronize(ev1));
     float ms = 0.f;
     ENG_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+    if (trace)
+        fprintf(stderr, "perft-trace %s sv=%s parents=%llu items=%llu..%llu grid=%d ms=%.4f\n",
+                mode == MODE_LEAF ? "leaf" : "expand", slider_name(sv), (unsigned long long)parents.n,
+                (unsigned long long)itemBase, (unsigned long long)itemEnd, grid, ms);
     if (mode == MODE_LEAF) {
         stats.leaf_launches++;
         stats.leaf_items += itemEnd - itemBase;
@@ -1045,9 +1065,9 @@ struct NoallocRun {
         const u64 nTiles = (total + TILE_CAP - 1) / TILE_CAP;
         if (cudaMemsetAsync(counter, 0, 4, st) != cudaSuccess) return PERFT_ERR_CUDA;
         if (mode == MODE_LEAF)
-            k_tile<MODE_LEAF, SV_KOGGE><<<(int)std::min<u64>(gridLeaf, nTiles), TILE_NT, 0, st>>>(P);
+            launch_tile_variant<MODE_LEAF>(SV_KOGGE, (int)std::min<u64>(gridLeaf, nTiles), st, P);
         else
-            k_tile<MODE_EXPAND, SV_KOGGE><<<(int)std::min<u64>(gridExpand, nTiles), TILE_NT, 0, st>>>(P);
+            launch_tile_variant<MODE_EXPAND>(SV_KOGGE, (int)std::min<u64>(gridExpand, nTiles), st, P);
         return cudaGetLastError() == cudaSuccess ? PERFT_OK : PERFT_ERR_CUDA;
     }
 

@@ -16,7 +16,8 @@ constexpr int CHAINS = 8;
 
 // kind 0: LOP3 (3-input logic), kind 1: integer add, kind 2: LOP3/add/SHF
 // mix, kind 3: IMAD (integer multiply-add, the FMA pipe), kind 4: LOP3 and
-// IMAD alternating (both integer pipes).  Inline PTX keeps the compiler from
+// IMAD alternating (both integer pipes), kind 5: IMAD.HI, kind 6: IMAD.WIDE
+// (plus the LOP3 that folds its two result words).  Inline PTX keeps the compiler from
 // folding the chains.
 template <int KIND>
 __global__ void __launch_bounds__(NT) k_probe(uint32_t *out, uint32_t seed, int iters)
@@ -38,9 +39,15 @@ __global__ void __launch_bounds__(NT) k_probe(uint32_t *out, uint32_t seed, int 
                 asm volatile("shf.l.wrap.b32 %0, %1, %2, 7;" : "=r"(r) : "r"(r), "r"(b));
             } else if (KIND == 3) {
                 asm volatile("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(r), "r"(b), "r"(c));
-            } else {
+            } else if (KIND == 4) {
                 asm volatile("lop3.b32 %0, %1, %2, %3, 0x96;" : "=r"(r) : "r"(r), "r"(b), "r"(c));
                 asm volatile("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(r), "r"(b), "r"(c));
+            } else if (KIND == 5) {
+                asm volatile("mad.hi.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(r), "r"(b), "r"(c));
+            } else {
+                uint64_t w;
+                asm volatile("mad.wide.u32 %0, %1, %2, %3;" : "=l"(w) : "r"(r), "r"(b), "l"((uint64_t)c));
+                r = (uint32_t)w ^ (uint32_t)(w >> 32);
             }
             a[i] = r;
         }
@@ -86,9 +93,9 @@ double run(int device, int opsPerChainStep)
 extern "C" {
 
 // Writes the measured 32-bit integer instructions per second (per lane) for
-// five instruction mixes: LOP3, add, LOP3+add+SHF, IMAD, LOP3+IMAD.
-// Returns 0 on success.
-int perft_int32_peak_probe(int device, double out[5])
+// seven instruction mixes: LOP3, add, LOP3+add+SHF, IMAD, LOP3+IMAD,
+// IMAD.HI, IMAD.WIDE+LOP3.  Returns 0 on success.
+int perft_int32_peak_probe(int device, double out[7])
 {
     if (cudaSetDevice(device) != cudaSuccess) return -1;
     out[0] = run<0>(device, 1);
@@ -96,7 +103,9 @@ int perft_int32_peak_probe(int device, double out[5])
     out[2] = run<2>(device, 3);
     out[3] = run<3>(device, 1);
     out[4] = run<4>(device, 2);
-    for (int i = 0; i < 5; i++)
+    out[5] = run<5>(device, 1);
+    out[6] = run<6>(device, 2);
+    for (int i = 0; i < 7; i++)
         if (out[i] <= 0) return -1;
     return 0;
 }

@@ -32,6 +32,12 @@
 
 #include <stdint.h>
 
+// Knight moves of the Kogge-Stone variants: 0 = eight jump shifts over the
+// whole knight set, 1 = one table lookup per knight.
+#ifndef PG_KNIGHT_LUT
+#define PG_KNIGHT_LUT 1
+#endif
+
 #ifdef __CUDACC__
 #define PG_HD __host__ __device__ __forceinline__
 #else
@@ -75,16 +81,18 @@ enum SliderVariant : int {
     SV_KOGGE = 0,      // occluded fills, all pieces of a set at once, no tables
     SV_MAGIC = 1,      // fancy magic lookups, one per piece
     SV_KOGGE_FMA = 2,  // occluded fills with every constant shift on the FMA pipe
-    SV_KOGGE_MIX = 3,  // FMA-pipe shifts for the opponent's attack map only
+    SV_KOGGE_SPLIT = 3,  // left shifts split: high word on the ALU, low word on the FMA pipe
     SV_COUNT = 4,
 };
+
+// How a Kogge-Stone fill issues its constant shifts.
+enum ShiftMode : int { SH_ALU = 0, SH_FMA = 1, SH_SPLIT = 2 };
 
 // Compile-time properties of a variant.
 template <int SV>
 struct SvTraits {
     static constexpr bool kogge = SV != SV_MAGIC;
-    static constexpr bool fmaAttack = SV == SV_KOGGE_FMA || SV == SV_KOGGE_MIX;
-    static constexpr bool fmaOwn = SV == SV_KOGGE_FMA;
+    static constexpr int shift = SV == SV_KOGGE_FMA ? SH_FMA : (SV == SV_KOGGE_SPLIT ? SH_SPLIT : SH_ALU);
 };
 
 // ------------------------------------------------------------------ tables
@@ -213,16 +221,34 @@ PG_HD u64 shr_fma(u64 x)
 #endif
 }
 
-template <int K, bool FMA>
+// Left shift with the high word from an ALU funnel shift and the low word
+// from an integer multiply (FMA pipe): one instruction on each pipe.
+template <int K>
+PG_HD u64 shl_split(u64 x)
+{
+#ifdef __CUDA_ARCH__
+    const u32 lo = (u32)x, hi = (u32)(x >> 32);
+    if (K == 0) return x;
+    if (K >= 32) return shl_fma<K>(x);
+    const u32 nhi = __funnelshift_l(lo, hi, K);
+    const u32 nlo = lo * c_pow2[K];
+    return ((u64)nhi << 32) | nlo;
+#else
+    return x << K;
+#endif
+}
+
+template <int K, int MODE>
 PG_HD u64 shl(u64 x)
 {
-    if (FMA) return shl_fma<K>(x);
+    if (MODE == SH_FMA) return shl_fma<K>(x);
+    if (MODE == SH_SPLIT) return shl_split<K>(x);
     return x << K;
 }
-template <int K, bool FMA>
+template <int K, int MODE>
 PG_HD u64 shr(u64 x)
 {
-    if (FMA) return shr_fma<K>(x);
+    if (MODE == SH_FMA) return shr_fma<K>(x);
     return x >> K;
 }
 
@@ -232,7 +258,7 @@ PG_HD u64 shr(u64 x)
 // fill is OR-distributive over generators, and same-direction rays of
 // different pieces never share a non-own square, so per-direction popcounts
 // of a whole piece set sum to the per-piece move counts.
-template <int S, bool LEFT, bool FMA>
+template <int S, bool LEFT, int FMA>
 PG_HD u64 ks_dir(u64 g, u64 p, u64 wrap)
 {
     p &= wrap;
@@ -253,21 +279,21 @@ PG_HD u64 ks_dir(u64 g, u64 p, u64 wrap)
     }
 }
 
-template <bool F = false> PG_HD u64 ks_north(u64 g, u64 p) { return ks_dir<8, true, F>(g, p, ~0ULL); }
-template <bool F = false> PG_HD u64 ks_south(u64 g, u64 p) { return ks_dir<8, false, F>(g, p, ~0ULL); }
-template <bool F = false> PG_HD u64 ks_east(u64 g, u64 p) { return ks_dir<1, true, F>(g, p, ~FILEA); }
-template <bool F = false> PG_HD u64 ks_west(u64 g, u64 p) { return ks_dir<1, false, F>(g, p, ~FILEH); }
-template <bool F = false> PG_HD u64 ks_ne(u64 g, u64 p) { return ks_dir<9, true, F>(g, p, ~FILEA); }
-template <bool F = false> PG_HD u64 ks_nw(u64 g, u64 p) { return ks_dir<7, true, F>(g, p, ~FILEH); }
-template <bool F = false> PG_HD u64 ks_se(u64 g, u64 p) { return ks_dir<7, false, F>(g, p, ~FILEA); }
-template <bool F = false> PG_HD u64 ks_sw(u64 g, u64 p) { return ks_dir<9, false, F>(g, p, ~FILEH); }
+template <int F = SH_ALU> PG_HD u64 ks_north(u64 g, u64 p) { return ks_dir<8, true, F>(g, p, ~0ULL); }
+template <int F = SH_ALU> PG_HD u64 ks_south(u64 g, u64 p) { return ks_dir<8, false, F>(g, p, ~0ULL); }
+template <int F = SH_ALU> PG_HD u64 ks_east(u64 g, u64 p) { return ks_dir<1, true, F>(g, p, ~FILEA); }
+template <int F = SH_ALU> PG_HD u64 ks_west(u64 g, u64 p) { return ks_dir<1, false, F>(g, p, ~FILEH); }
+template <int F = SH_ALU> PG_HD u64 ks_ne(u64 g, u64 p) { return ks_dir<9, true, F>(g, p, ~FILEA); }
+template <int F = SH_ALU> PG_HD u64 ks_nw(u64 g, u64 p) { return ks_dir<7, true, F>(g, p, ~FILEH); }
+template <int F = SH_ALU> PG_HD u64 ks_se(u64 g, u64 p) { return ks_dir<7, false, F>(g, p, ~FILEA); }
+template <int F = SH_ALU> PG_HD u64 ks_sw(u64 g, u64 p) { return ks_dir<9, false, F>(g, p, ~FILEH); }
 
-template <bool F = false>
+template <int F = SH_ALU>
 PG_HD u64 ks_diag(u64 g, u64 empty)
 {
     return ks_ne<F>(g, empty) | ks_nw<F>(g, empty) | ks_se<F>(g, empty) | ks_sw<F>(g, empty);
 }
-template <bool F = false>
+template <int F = SH_ALU>
 PG_HD u64 ks_orth(u64 g, u64 empty)
 {
     return ks_north<F>(g, empty) | ks_south<F>(g, empty) | ks_east<F>(g, empty) | ks_west<F>(g, empty);
@@ -275,13 +301,13 @@ PG_HD u64 ks_orth(u64 g, u64 empty)
 
 // Per-direction move counts of a whole slider set (targets = squares the
 // pieces may land on).
-template <bool F = false>
+template <int F = SH_ALU>
 PG_HD int ks_count_diag(u64 g, u64 empty, u64 targets)
 {
     return popc(ks_ne<F>(g, empty) & targets) + popc(ks_nw<F>(g, empty) & targets) +
            popc(ks_se<F>(g, empty) & targets) + popc(ks_sw<F>(g, empty) & targets);
 }
-template <bool F = false>
+template <int F = SH_ALU>
 PG_HD int ks_count_orth(u64 g, u64 empty, u64 targets)
 {
     return popc(ks_north<F>(g, empty) & targets) + popc(ks_south<F>(g, empty) & targets) +
@@ -305,20 +331,20 @@ template <int SV>
 PG_HD u64 bishop_att(int sq, u64 occ)
 {
     if (SV == SV_MAGIC) return magic_bishop(sq, occ);
-    return ks_diag<SvTraits<SV>::fmaOwn>(1ULL << sq, ~occ);
+    return ks_diag<SvTraits<SV>::shift>(1ULL << sq, ~occ);
 }
 template <int SV>
 PG_HD u64 rook_att(int sq, u64 occ)
 {
     if (SV == SV_MAGIC) return magic_rook(sq, occ);
-    return ks_orth<SvTraits<SV>::fmaOwn>(1ULL << sq, ~occ);
+    return ks_orth<SvTraits<SV>::shift>(1ULL << sq, ~occ);
 }
 
 // Union of the attacks of a slider set; occ excludes transparent squares.
 template <int SV>
 PG_HD u64 bishop_set_att(u64 set, u64 occ)
 {
-    if (SvTraits<SV>::kogge) return ks_diag<SvTraits<SV>::fmaAttack>(set, ~occ);
+    if (SvTraits<SV>::kogge) return ks_diag<SvTraits<SV>::shift>(set, ~occ);
     u64 a = 0;
     while (set) {
         a |= magic_bishop(ctz(set), occ);
@@ -329,7 +355,7 @@ PG_HD u64 bishop_set_att(u64 set, u64 occ)
 template <int SV>
 PG_HD u64 rook_set_att(u64 set, u64 occ)
 {
-    if (SvTraits<SV>::kogge) return ks_orth<SvTraits<SV>::fmaAttack>(set, ~occ);
+    if (SvTraits<SV>::kogge) return ks_orth<SvTraits<SV>::shift>(set, ~occ);
     u64 a = 0;
     while (set) {
         a |= magic_rook(ctz(set), occ);
@@ -511,7 +537,7 @@ PG_HD u32 count_moves(const Board &b)
 
     // knights
     const u64 N = b.knights & c.mine & ~pinned;
-    if (SvTraits<SV>::kogge) {
+    if (SvTraits<SV>::kogge && !PG_KNIGHT_LUT) {
         n += knight_set_count(N, targets);
     } else {
         u64 k = N;
@@ -525,7 +551,7 @@ PG_HD u32 count_moves(const Board &b)
     const u64 B = b.bq & c.mine & ~pinned;
     const u64 R = b.rq & c.mine & ~pinned;
     if (SvTraits<SV>::kogge) {
-        constexpr bool F = SvTraits<SV>::fmaOwn;
+        constexpr int F = SvTraits<SV>::shift;
         n += ks_count_diag<F>(B, c.empty, targets) + ks_count_orth<F>(R, c.empty, targets);
     } else {
         u64 x = B;
