@@ -158,10 +158,19 @@ typedef struct perft_stats {
     uint64_t arena_bytes;
     uint64_t peak_arena_bytes;
     uint32_t chunked_levels;     /* levels split to fit the arena */
+    uint64_t tt_entries;         /* transposition-table size (0: no table) */
+    uint64_t tt_probes;          /* nodes looked up */
+    uint64_t tt_hits;            /* lookups answered by the table */
+    uint64_t tt_duplicates;      /* same-level transpositions expanded once */
+    uint64_t tt_stores;          /* entries written */
 } perft_stats;
 
 int perft_get_stats(perft_stats *out);
 int perft_reset_stats(void);
+
+/* Empties the transposition table (entries stay valid across calls, since a
+ * position's perft never changes; clearing only matters for timing). */
+int perft_tt_clear(void);
 
 #ifdef __cplusplus
 }

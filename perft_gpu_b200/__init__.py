@@ -82,6 +82,11 @@ class PerftStats(ctypes.Structure):
         ("arena_bytes", ctypes.c_uint64),
         ("peak_arena_bytes", ctypes.c_uint64),
         ("chunked_levels", ctypes.c_uint32),
+        ("tt_entries", ctypes.c_uint64),
+        ("tt_probes", ctypes.c_uint64),
+        ("tt_hits", ctypes.c_uint64),
+        ("tt_duplicates", ctypes.c_uint64),
+        ("tt_stores", ctypes.c_uint64),
     ]
 
 
@@ -114,6 +119,7 @@ def _load():
         "perft_position_features": (ctypes.c_int, [P(_Pos48), P(ctypes.c_uint32)]),
         "perft_get_stats": (ctypes.c_int, [P(PerftStats)]),
         "perft_reset_stats": (ctypes.c_int, []),
+        "perft_tt_clear": (ctypes.c_int, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -122,16 +128,21 @@ def _load():
     return lib
 
 
-_lib = _load()
+_lib_handle = None
 
 
 def lib():
-    """The loaded ctypes library (for callers that want raw access)."""
-    return _lib
+    """The loaded ctypes library.  Loaded on first use, so the package (and
+    its build module) imports before the library has been built; every
+    engine call fails loudly if the library is missing."""
+    global _lib_handle
+    if _lib_handle is None:
+        _lib_handle = _load()
+    return _lib_handle
 
 
 def _status_string(status: int) -> str:
-    s = _lib.perft_status_string(int(status))
+    s = lib().perft_status_string(int(status))
     return s.decode() if s else "unknown"
 
 
@@ -157,7 +168,7 @@ def config(device: int = 0, arena_bytes: int = 0, sliders_expand: int = SLIDERS_
            sliders_leaf: int = SLIDERS_AUTO, tt_log2_entries: int = 0,
            zobrist_seed: int | None = None) -> PerftConfig:
     cfg = PerftConfig()
-    _lib.perft_config_default(ctypes.byref(cfg))
+    lib().perft_config_default(ctypes.byref(cfg))
     cfg.device = device
     cfg.arena_bytes = arena_bytes
     cfg.sliders_expand = sliders_expand
@@ -169,19 +180,19 @@ def config(device: int = 0, arena_bytes: int = 0, sliders_expand: int = SLIDERS_
 
 
 def init(device: int = 0, arena_bytes: int = 0, sliders_expand: int = SLIDERS_AUTO,
-         sliders_leaf: int = SLIDERS_AUTO, tt_log2_entries: int = 0) -> None:
-    cfg = config(device, arena_bytes, sliders_expand, sliders_leaf, tt_log2_entries)
-    _check(_lib.perft_init(ctypes.byref(cfg)), "perft_init")
+         sliders_leaf: int = SLIDERS_AUTO, tt_log2_entries: int = 0, zobrist_seed: int | None = None) -> None:
+    cfg = config(device, arena_bytes, sliders_expand, sliders_leaf, tt_log2_entries, zobrist_seed)
+    _check(lib().perft_init(ctypes.byref(cfg)), "perft_init")
 
 
 def shutdown() -> None:
-    _lib.perft_shutdown()
+    lib().perft_shutdown()
 
 
 def perft(pos, depth: int) -> int:
     out = ctypes.c_uint64(0)
     p = _pos(pos)
-    _check(_lib.perft(ctypes.byref(p), int(depth), ctypes.byref(out)), "perft")
+    _check(lib().perft(ctypes.byref(p), int(depth), ctypes.byref(out)), "perft")
     return int(out.value)
 
 
@@ -190,14 +201,14 @@ def perft_batch(positions, depths) -> np.ndarray:
     n = pos.shape[0]
     d = np.ascontiguousarray(np.broadcast_to(np.asarray(depths, dtype=np.uint8), (n,)))
     out = np.zeros(n, dtype=np.uint64)
-    _check(_lib.perft_batch(pos.ctypes.data, d.ctypes.data, n, out.ctypes.data), "perft_batch")
+    _check(lib().perft_batch(pos.ctypes.data, d.ctypes.data, n, out.ctypes.data), "perft_batch")
     return out
 
 
 def perft_batch_device(d_pos_ptr: int, depths, n: int, d_out_ptr: int) -> None:
     """Batched perft on device-resident buffers (e.g. torch CUDA tensors' data_ptr())."""
     d = np.ascontiguousarray(np.broadcast_to(np.asarray(depths, dtype=np.uint8), (n,)))
-    _check(_lib.perft_batch_device(ctypes.c_void_p(d_pos_ptr), d.ctypes.data, n,
+    _check(lib().perft_batch_device(ctypes.c_void_p(d_pos_ptr), d.ctypes.data, n,
                                    ctypes.c_void_p(d_out_ptr)), "perft_batch_device")
 
 
@@ -206,7 +217,7 @@ def divide(pos, depth: int) -> dict:
     moves = (ctypes.c_char * (6 * 256))()
     counts = (ctypes.c_uint64 * 256)()
     n = ctypes.c_uint32(0)
-    _check(_lib.perft_divide(ctypes.byref(p), int(depth), moves, counts, ctypes.byref(n)), "perft_divide")
+    _check(lib().perft_divide(ctypes.byref(p), int(depth), moves, counts, ctypes.byref(n)), "perft_divide")
     raw = bytes(moves)
     res = {}
     for i in range(n.value):
@@ -217,25 +228,29 @@ def divide(pos, depth: int) -> dict:
 
 def stats() -> dict:
     s = PerftStats()
-    _check(_lib.perft_get_stats(ctypes.byref(s)), "perft_get_stats")
+    _check(lib().perft_get_stats(ctypes.byref(s)), "perft_get_stats")
     return {name: getattr(s, name) for name, _ in PerftStats._fields_}
 
 
 def reset_stats() -> None:
-    _lib.perft_reset_stats()
+    lib().perft_reset_stats()
+
+
+def tt_clear() -> None:
+    _check(lib().perft_tt_clear(), "perft_tt_clear")
 
 
 # ------------------------------------------------------- host utilities
 def fen_to_pos(fen: str) -> np.ndarray:
     p = _Pos48()
-    _check(_lib.perft_fen_to_pos(fen.encode(), ctypes.byref(p)), f"fen_to_pos({fen!r})")
+    _check(lib().perft_fen_to_pos(fen.encode(), ctypes.byref(p)), f"fen_to_pos({fen!r})")
     return _arr(p)
 
 
 def pos_to_fen(pos) -> str:
     buf = ctypes.create_string_buffer(128)
     p = _pos(pos)
-    _check(_lib.perft_pos_to_fen(ctypes.byref(p), buf, 128), "pos_to_fen")
+    _check(lib().perft_pos_to_fen(ctypes.byref(p), buf, 128), "pos_to_fen")
     return buf.value.decode()
 
 
@@ -243,14 +258,14 @@ def legal_moves(pos) -> List[str]:
     buf = ctypes.create_string_buffer(6 * 256)
     n = ctypes.c_uint32(0)
     p = _pos(pos)
-    _check(_lib.perft_legal_moves_uci(ctypes.byref(p), buf, len(buf), ctypes.byref(n)), "legal_moves")
+    _check(lib().perft_legal_moves_uci(ctypes.byref(p), buf, len(buf), ctypes.byref(n)), "legal_moves")
     s = buf.value.decode()
     return s.split() if s else []
 
 
 def apply_move(pos, uci: str) -> np.ndarray:
     p = _pos(pos)
-    _check(_lib.perft_apply_uci_move(ctypes.byref(p), uci.encode()), f"apply_move({uci})")
+    _check(lib().perft_apply_uci_move(ctypes.byref(p), uci.encode()), f"apply_move({uci})")
     return _arr(p)
 
 
@@ -263,7 +278,7 @@ def position_from_moves(fen: str, moves: Iterable[str]) -> np.ndarray:
 
 def random_playouts(seed: int, n: int, min_plies: int, max_plies: int) -> np.ndarray:
     out = np.zeros((n, 6), dtype=np.uint64)
-    _check(_lib.perft_random_playouts(seed, n, min_plies, max_plies, out.ctypes.data), "random_playouts")
+    _check(lib().perft_random_playouts(seed, n, min_plies, max_plies, out.ctypes.data), "random_playouts")
     return out
 
 
@@ -277,7 +292,7 @@ FEATURE_PROMOTION = 16
 def features(pos) -> int:
     p = _pos(pos)
     f = ctypes.c_uint32(0)
-    _check(_lib.perft_position_features(ctypes.byref(p), ctypes.byref(f)), "features")
+    _check(lib().perft_position_features(ctypes.byref(p), ctypes.byref(f)), "features")
     return int(f.value)
 
 

@@ -77,8 +77,10 @@ constexpr u32 DERR_BAD_POSITION = 4u;
 
 enum { MODE_EXPAND = 0, MODE_LEAF = 1 };
 
-// Bytes of one level node: 6 planes + count + root + scan entry.
-constexpr u64 NODE_BYTES = 6 * 8 + 4 + 4 + 8;
+// Bytes of one level node: 6 planes + count + root + scan entry, plus its
+// share of the tile index (4 B per TILE_CAP items, up to 218 items a node)
+// and of the scan's block sums, rounded up.
+constexpr u64 NODE_BYTES = 6 * 8 + 4 + 4 + 8 + 1;
 
 // --------------------------------------------------------- block helpers
 template <int NT>
@@ -232,7 +234,7 @@ struct TileParams {
     const u64 *ppl;   // parent planes, plane i at ppl + i * pstride
     u64 pstride;
     const u64 *pscan; // nParents + 1 item offsets
-    const u32 *proot;
+    const u32 *proot;  // root id of each parent; null: sums go to the parent's own slot
     u64 nParents;
     const u32 *tileFirst;  // indexed by absolute tile number
     u64 itemBase;     // first item of this launch (multiple of TILE_CAP)
@@ -300,7 +302,7 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams P)
                 qEnd = P.pscan[q + 1];
 #pragma unroll
                 for (int k = 0; k < 6; k++) sb[k][tid] = P.ppl[k * P.pstride + q];
-                sroot[tid] = P.proot[q];
+                sroot[tid] = P.proot ? P.proot[q] : (u32)q;  // no root array: account to the parent itself
             }
             const u64 sBeg = max(P.pscan[p], iBeg);
             const u64 sEnd = min(P.pscan[p + nP], iEnd);
@@ -319,7 +321,8 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams P)
             }
 
             // ---- generate the window's moves into the shared item list
-            if (valid && qEnd > sBeg && qBeg < sEnd) {
+            // parents without items (none legal, or answered by the table) generate nothing
+            if (valid && qEnd > qBeg && qEnd > sBeg && qBeg < sEnd) {
                 const Board b{sb[0][tid], sb[1][tid], sb[2][tid], sb[3][tid], sb[4][tid], sb[5][tid]};
                 WindowSink sink{sitems, qBeg, sBeg, sEnd, (u32)tid << 16};
                 gen_moves<SV>(b, sink);
@@ -374,14 +377,200 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams P)
     }
 }
 
+// ====================================================== transposition table
+// Lockless table of 16-byte entries {key ^ value, value}: a torn or foreign
+// entry fails the XOR check (the reference's scheme, perft_bb.h:759-764,
+// with 64-bit keys).  Keys are Zobrist hashes of the side-relative board
+// (781 seeded keys: 12 piece kinds x 64 squares, 4 castling rights, 8
+// en-passant files, one spare) XOR a per-remaining-depth key, so one table
+// holds every depth ("per-depth slots").  Perft is invariant under the
+// colour mirror, so a position and its mirror may share an entry.
+constexpr int ZOB_KEYS = 781;
+constexpr int ZOB_DEPTH_KEYS = 32;
+__device__ u64 d_zobrist[ZOB_KEYS + ZOB_DEPTH_KEYS];
+
+constexpr u32 ALIAS_HIT = 0xFFFFFFFFu;     // value came from the table
+constexpr u32 ALIAS_NOSLOT = 0xFFFFFFFEu;  // not de-duplicated (set full)
+constexpr u64 DEDUP_EMPTY = ~0ULL;
+constexpr int DEDUP_MAX_PROBES = 64;
+
+struct TTStats {
+    unsigned long long probes, hits, aliases, stores;
+};
+
+__device__ __forceinline__ u64 zobrist_rel(const Board &b)
+{
+    const u64 pawns = b.pawns & RANKS2TO7;
+    const u64 occ = pawns | b.knights | b.bq | b.rq | b.kings;
+    const u64 theirs = occ ^ b.mine;
+    const u64 sets[6] = {pawns, b.knights, b.bq & ~b.rq, b.rq & ~b.bq, b.bq & b.rq, b.kings};
+    u64 h = 0;
+#pragma unroll
+    for (int pc = 0; pc < 6; pc++) {
+        u64 m = sets[pc] & b.mine;
+        while (m) {
+            h ^= __ldg(&d_zobrist[pc * 64 + ctz(m)]);
+            m &= m - 1;
+        }
+        u64 t = sets[pc] & theirs;
+        while (t) {
+            h ^= __ldg(&d_zobrist[(6 + pc) * 64 + ctz(t)]);
+            t &= t - 1;
+        }
+    }
+    const u32 st = (u32)(b.pawns & 0xFF);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (st & (1u << k)) h ^= __ldg(&d_zobrist[768 + k]);
+    if (st >> 4) h ^= __ldg(&d_zobrist[772 + (st >> 4) - 1]);
+    return h;
+}
+
+// Warp-aggregated increment of a statistics counter.
+__device__ __forceinline__ void count_stat(unsigned long long *ctr, bool hit)
+{
+    const unsigned m = __ballot_sync(__activemask(), hit);
+    if (m && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(ctr, (unsigned long long)__popc(m));
+}
+
+// Hash every node, probe the table, and insert misses into the level's
+// de-duplication set (lowest index wins).  Hits get their value and no
+// children; their alias is ALIAS_HIT.  Misses keep the set slot in alias.
+__global__ void __launch_bounds__(256) k_tt_probe(const u64 *__restrict__ planes, u64 stride, u64 n, int remaining,
+                                                  bool probe, u32 *__restrict__ cnt, u64 *__restrict__ hash,
+                                                  unsigned long long *__restrict__ acc, u32 *__restrict__ alias,
+                                                  const ulonglong2 *tt, u64 ttMask, u64 *__restrict__ dkey,
+                                                  u32 *__restrict__ downer, u64 dMask, TTStats *ts)
+{
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    bool hit = false;
+    if (i < n) {
+        const Board b{planes[i], planes[stride + i], planes[2 * stride + i], planes[3 * stride + i],
+                      planes[4 * stride + i], planes[5 * stride + i]};
+        const u64 h = zobrist_rel(b) ^ __ldg(&d_zobrist[ZOB_KEYS + remaining]);
+        hash[i] = h;
+        acc[i] = 0;
+        if (probe) {
+            const ulonglong2 e = tt[h & ttMask];
+            if ((e.x ^ e.y) == h) {
+                hit = true;
+                acc[i] = e.y;
+                cnt[i] = 0;
+                alias[i] = ALIAS_HIT;
+            }
+        }
+        if (!hit) {
+            u32 placed = ALIAS_NOSLOT;
+            if (h != DEDUP_EMPTY) {
+                u64 slot = (h * 0x9E3779B97F4A7C15ULL >> 17) & dMask;
+                for (int k = 0; k < DEDUP_MAX_PROBES; k++) {
+                    const unsigned long long old =
+                        atomicCAS((unsigned long long *)&dkey[slot], (unsigned long long)DEDUP_EMPTY,
+                                  (unsigned long long)h);
+                    if (old == DEDUP_EMPTY || old == h) {
+                        atomicMin(&downer[slot], (u32)i);
+                        placed = (u32)slot;
+                        break;
+                    }
+                    slot = (slot + 1) & dMask;
+                }
+            }
+            alias[i] = placed;
+        }
+    }
+    if (probe) {
+        count_stat(&ts->probes, i < n);
+        count_stat(&ts->hits, hit);
+    }
+}
+
+// Turns set slots into owner indices; duplicates lose their children.
+__global__ void __launch_bounds__(256) k_tt_dedup(u64 n, u32 *__restrict__ cnt, u32 *__restrict__ alias,
+                                                  const u32 *__restrict__ downer, TTStats *ts)
+{
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    bool dup = false;
+    if (i < n) {
+        const u32 a = alias[i];
+        if (a != ALIAS_HIT && a != ALIAS_NOSLOT) {
+            const u32 o = downer[a];
+            alias[i] = o;
+            if (o != (u32)i) {
+                cnt[i] = 0;
+                dup = true;
+            }
+        }
+    }
+    count_stat(&ts->aliases, dup);
+}
+
+// After a level's subtrees are summed into acc: copy owners' values into
+// their duplicates, store owners in the table, and add every value into the
+// parent level (nodes are ordered by parent: segmented warp sums, then one
+// atomic per parent run).  At level 0 the values go to the roots' results.
+__global__ void __launch_bounds__(256) k_tt_finish(u64 n, bool store, const u64 *__restrict__ hash,
+                                                   unsigned long long *__restrict__ acc, const u32 *__restrict__ alias,
+                                                   const u32 *__restrict__ parent, unsigned long long *parentAcc,
+                                                   ulonglong2 *tt, u64 ttMask, TTStats *ts)
+{
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    unsigned long long v = 0;
+    u32 key = 0xFFFFFFFFu;
+    bool stored = false;
+    if (i < n) {
+        const u32 a = alias[i];
+        v = acc[i];
+        if (a != ALIAS_HIT && a != ALIAS_NOSLOT && a != (u32)i) {
+            v = acc[a];  // the owner is final: its subtree finished before this kernel
+        } else if (a != ALIAS_HIT && store) {
+            tt[hash[i] & ttMask] = make_ulonglong2(hash[i] ^ v, v);
+            stored = true;
+        }
+        key = parent[i];
+    }
+    count_stat(&ts->stores, stored);
+    if (!parentAcc) return;  // level 0: k_tt_roots writes the results
+    // segmented inclusive sum over runs of equal parent within the warp
+    unsigned long long sum = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, sum, o);
+        const u32 ky = __shfl_up_sync(0xffffffffu, key, o);
+        if (lane >= o && ky == key) sum += y;
+    }
+    const u32 knext = __shfl_down_sync(0xffffffffu, key, 1);
+    const bool last = (lane == 31) || knext != key;
+    if (i < n && last && key != 0xFFFFFFFFu) atomicAdd(&parentAcc[key], sum);
+}
+
+// Level 0 of a TT run: each root's value (own, owner's, or table's) is its result.
+__global__ void k_tt_roots(u64 n, const unsigned long long *__restrict__ acc, const u32 *__restrict__ alias,
+                           const u32 *__restrict__ root, unsigned long long *__restrict__ out)
+{
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const u32 a = alias[i];
+    out[root[i]] = (a != ALIAS_HIT && a != ALIAS_NOSLOT && a != (u32)i) ? acc[a] : acc[i];
+}
+
 // ================================================================ host side
 struct DeviceLevel {
     u64 *planes;
     u64 stride;
     u32 *cnt;
-    u32 *root;
+    u32 *root;  // root id (no TT) or parent index in the previous level (TT)
     u64 n;
+    // transposition-table runs only
+    u64 *hash = nullptr;
+    unsigned long long *acc = nullptr;  // perft of each node's subtree
+    u32 *alias = nullptr;               // owner index, ALIAS_HIT or ALIAS_NOSLOT
 };
+
+// Bytes of one TT level node: the plain node plus hash, subtree sum, alias,
+// and the transient de-duplication set (at most 2.5 slots of 12 bytes per
+// node; it is released before the scan, so this over-counts slightly).
+constexpr u64 NODE_BYTES_TT = NODE_BYTES + 8 + 8 + 4 + 30;
 
 class Engine {
 public:
@@ -422,6 +611,33 @@ private:
     int launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst,
                     u64 itemBase, u64 itemEnd, DeviceLevel *children, unsigned long long *rootCounts);
     int process_level(const DeviceLevel &L, int remaining, unsigned long long *rootCounts);
+    int process_level_tt(const DeviceLevel &L, int remaining, unsigned long long *parentAcc,
+                         unsigned long long *rootOut);
+    bool alloc_level_tt(DeviceLevel &L, u64 n);
+
+public:
+    int tt_clear();
+    void read_tt_stats()
+    {
+        TTStats t{};
+        if (dTTStats && cudaMemcpy(&t, dTTStats, sizeof t, cudaMemcpyDeviceToHost) == cudaSuccess) {
+            stats.tt_probes = t.probes;
+            stats.tt_hits = t.hits;
+            stats.tt_duplicates = t.aliases;
+            stats.tt_stores = t.stores;
+        }
+        stats.tt_entries = tt ? ttMask + 1 : 0;
+    }
+    void zero_tt_stats()
+    {
+        if (dTTStats) cudaMemset(dTTStats, 0, sizeof(TTStats));
+    }
+
+private:
+    ulonglong2 *tt = nullptr;
+    u64 ttMask = 0;
+    TTStats *dTTStats = nullptr;
+    int ttMinDepth = 2;
     int check(cudaError_t e, const char *what);
     int sync_and_check_errors();
     int autotune(bool leaf, bool expand);
@@ -508,6 +724,29 @@ int Engine::init(const perft_config &cfg)
     ENG_TRY(cudaMalloc(&dErr, 64));
     ENG_TRY(cudaMallocHost(&hPinned, 64));
 
+    // Zobrist keys (splitmix64 of the seed) and the transposition table
+    {
+        u64 keys[ZOB_KEYS + ZOB_DEPTH_KEYS];
+        u64 x = cfg.zobrist_seed;
+        for (int k = 0; k < ZOB_KEYS + ZOB_DEPTH_KEYS; k++) {
+            x += 0x9E3779B97F4A7C15ULL;
+            u64 z = x;
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+            keys[k] = z ^ (z >> 31);
+        }
+        ENG_TRY(cudaMemcpyToSymbol(d_zobrist, keys, sizeof keys));
+    }
+    ENG_TRY(cudaMalloc(&dTTStats, sizeof(TTStats)));
+    ENG_TRY(cudaMemset(dTTStats, 0, sizeof(TTStats)));
+    if (cfg.tt_log2_entries > 0) {
+        if (cfg.tt_log2_entries < 10 || cfg.tt_log2_entries > 34) return PERFT_ERR_INVALID_ARG;
+        const u64 entries = 1ULL << cfg.tt_log2_entries;
+        ENG_TRY(cudaMalloc(&tt, entries * sizeof(ulonglong2)));
+        ENG_TRY(cudaMemset(tt, 0, entries * sizeof(ulonglong2)));
+        ttMask = entries - 1;
+    }
+
     size_t freeB = 0, totalB = 0;
     ENG_TRY(cudaMemGetInfo(&freeB, &totalB));
     u64 want = cfg.arena_bytes ? cfg.arena_bytes : (u64)(freeB * 0.85);
@@ -550,6 +789,11 @@ void Engine::shutdown()
     cudaSetDevice(device);
     cudaStreamSynchronize(stream);
     cudaFree(arena);
+    if (tt) cudaFree(tt);
+    tt = nullptr;
+    ttMask = 0;
+    if (dTTStats) cudaFree(dTTStats);
+    dTTStats = nullptr;
     cudaFree(dCounter);
     cudaFree(dErr);
     cudaFreeHost(hPinned);
@@ -701,6 +945,12 @@ int Engine::autotune(bool leaf, bool expand)
     if (!dPos || !dOut) return PERFT_ERR_OUT_OF_MEMORY;
     ENG_TRY(cudaMemcpyAsync(dPos, pos.data(), 48ull * N, cudaMemcpyHostToDevice, stream));
     const int keepLeaf = svLeaf, keepExpand = svExpand;
+    ulonglong2 *keepTT = tt;
+    tt = nullptr;  // time the kernels, not table hits
+    struct Restore {
+        ulonglong2 *&slot, *value;
+        ~Restore() { slot = value; }
+    } restore{tt, keepTT};
     auto timed = [&](int l, int e, double &leafMs, double &expandMs) -> int {
         svLeaf = l;
         svExpand = e;
@@ -732,7 +982,97 @@ int Engine::autotune(bool leaf, bool expand)
     }
     svLeaf = bestLeaf;
     svExpand = bestExpand;
+    tt = keepTT;
     arenaTop = mark;
+    return PERFT_OK;
+}
+
+bool Engine::alloc_level_tt(DeviceLevel &L, u64 n)
+{
+    if (!alloc_level(L, n)) return false;
+    L.hash = (u64 *)alloc(8 * L.stride);
+    L.acc = (unsigned long long *)alloc(8 * L.stride);
+    L.alias = (u32 *)alloc(4 * L.stride);
+    return L.hash && L.acc && L.alias;
+}
+
+int Engine::tt_clear()
+{
+    if (tt) ENG_TRY(cudaMemsetAsync(tt, 0, (ttMask + 1) * sizeof(ulonglong2), stream));
+    ENG_TRY(cudaMemsetAsync(dTTStats, 0, sizeof(TTStats), stream));
+    ENG_TRY(cudaStreamSynchronize(stream));
+    return PERFT_OK;
+}
+
+// Transposition-table version of process_level.  Every node of L (remaining
+// plies `remaining`) is hashed and probed; hits and same-level duplicates
+// are not expanded.  Subtree sums accumulate in L.acc: directly from the
+// count-only last ply, or from the child levels' finish pass.  When L is
+// done, owners are stored, duplicates copy their owner's value, and the
+// values are added into parentAcc (or written to the roots' results).
+int Engine::process_level_tt(const DeviceLevel &L, int remaining, unsigned long long *parentAcc,
+                             unsigned long long *rootOut)
+{
+    if (L.n == 0) return PERFT_OK;
+    const u64 mark = arenaTop;
+    const unsigned nb = (unsigned)((L.n + 255) / 256);
+    const bool useTT = remaining >= ttMinDepth;
+
+    u64 dsize = 1024;
+    while (dsize < L.n + L.n / 4) dsize <<= 1;  // load <= 80%; unplaced nodes are simply not de-duplicated
+    u64 *dkey = (u64 *)alloc(8 * dsize);
+    u32 *downer = (u32 *)alloc(4 * dsize);
+    if (!dkey || !downer) return PERFT_ERR_OUT_OF_MEMORY;
+    ENG_TRY(cudaMemsetAsync(dkey, 0xFF, 8 * dsize, stream));
+    ENG_TRY(cudaMemsetAsync(downer, 0xFF, 4 * dsize, stream));
+    k_tt_probe<<<nb, 256, 0, stream>>>(L.planes, L.stride, L.n, remaining, useTT, L.cnt, L.hash, L.acc, L.alias,
+                                       tt, ttMask, dkey, downer, dsize - 1, dTTStats);
+    k_tt_dedup<<<nb, 256, 0, stream>>>(L.n, L.cnt, L.alias, downer, dTTStats);
+    stats.other_launches += 2;
+    ENG_TRY(cudaGetLastError());
+    arenaTop = mark;  // the de-duplication set is no longer needed
+
+    u64 *pscan = nullptr;
+    u32 *tileFirst = nullptr;
+    u64 total = 0;
+    int rc = scan(L.cnt, L.n, pscan, tileFirst, total);
+    if (rc != PERFT_OK) return rc;
+    DeviceLevel self = L;
+    self.root = nullptr;  // tile sums and child links point at the parent itself
+    if (total > 0) {
+        if (remaining == 2) {
+            rc = launch_tile(MODE_LEAF, self, pscan, tileFirst, 0, total, nullptr, L.acc);
+            if (rc != PERFT_OK) return rc;
+        } else {
+            const u64 slack = std::min<u64>(64ull << 20, arenaCap / 16);
+            const u64 freeB = arena_free() > slack ? arena_free() - slack : 0;
+            u64 budgetNodes = freeB / NODE_BYTES_TT;
+            if (remaining > 3) budgetNodes /= 2;
+            const u64 chunk = total <= budgetNodes ? total : (budgetNodes & ~(u64)(TILE_CAP - 1));
+            if (chunk == 0) return PERFT_ERR_OUT_OF_MEMORY;
+            if (chunk < total) stats.chunked_levels++;
+            for (u64 lo = 0; lo < total; lo += chunk) {
+                const u64 hi = std::min(total, lo + chunk);
+                const u64 cm = arenaTop;
+                DeviceLevel C;
+                if (!alloc_level_tt(C, hi - lo)) return PERFT_ERR_OUT_OF_MEMORY;
+                rc = launch_tile(MODE_EXPAND, self, pscan, tileFirst, lo, hi, &C, nullptr);
+                if (rc != PERFT_OK) return rc;
+                rc = process_level_tt(C, remaining - 1, L.acc, nullptr);
+                if (rc != PERFT_OK) return rc;
+                arenaTop = cm;
+            }
+        }
+    }
+    arenaTop = mark;
+    k_tt_finish<<<nb, 256, 0, stream>>>(L.n, useTT && tt != nullptr, L.hash, L.acc, L.alias, L.root, parentAcc, tt,
+                                        ttMask, dTTStats);
+    stats.other_launches++;
+    if (rootOut) {
+        k_tt_roots<<<nb, 256, 0, stream>>>(L.n, L.acc, L.alias, L.root, rootOut);
+        stats.other_launches++;
+    }
+    ENG_TRY(cudaGetLastError());
     return PERFT_OK;
 }
 
@@ -765,7 +1105,7 @@ int Engine::run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut)
         const u64 gm = arenaTop;
         u32 *dIds = (u32 *)alloc(4ull * ids.size());
         DeviceLevel L0;
-        if (!dIds || !alloc_level(L0, ids.size())) {
+        if (!dIds || !(tt ? alloc_level_tt(L0, ids.size()) : alloc_level(L0, ids.size()))) {
             rc = PERFT_ERR_OUT_OF_MEMORY;
             break;
         }
@@ -777,7 +1117,7 @@ int Engine::run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut)
         ENG_TRY(cudaGetLastError());
         rc = sync_and_check_errors();
         if (rc != PERFT_OK) break;
-        if (depth >= 2) rc = process_level(L0, depth, rootCounts);
+        if (depth >= 2) rc = tt ? process_level_tt(L0, depth, nullptr, rootCounts) : process_level(L0, depth, rootCounts);
         arenaTop = gm;
         if (rc != PERFT_OK) break;
     }
@@ -904,13 +1244,22 @@ int perft_get_stats(perft_stats *out)
 {
     if (!out) return PERFT_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(g_engine.mu);
+    if (g_engine.ready) g_engine.read_tt_stats();
     *out = g_engine.stats;
     return PERFT_OK;
+}
+
+int perft_tt_clear(void)
+{
+    std::lock_guard<std::mutex> lk(g_engine.mu);
+    if (!g_engine.ready) return PERFT_ERR_NOT_INITIALIZED;
+    return g_engine.tt_clear();
 }
 
 int perft_reset_stats(void)
 {
     std::lock_guard<std::mutex> lk(g_engine.mu);
+    if (g_engine.ready) g_engine.zero_tt_stats();
     perft_stats keep = g_engine.stats;
     memset(&g_engine.stats, 0, sizeof g_engine.stats);
     g_engine.stats.sliders_expand = keep.sliders_expand;
