@@ -29,6 +29,7 @@ extern "C" {
 
 /* ------------------------------------------------------------ status codes */
 #define PERFT_OK                   0
+#define PERFT_PENDING              1  /* serving: the query is still running */
 #define PERFT_ERR_INVALID_ARG     -1
 #define PERFT_ERR_NOT_INITIALIZED -2
 #define PERFT_ERR_CUDA            -3
@@ -118,6 +119,38 @@ int perft_divide(const perft_pos48 *pos, uint32_t depth, char (*moves)[6], uint6
 #define PERFT_NOALLOC_SCRATCH_BYTES (32ull << 20)
 int perft_batch_noalloc(const perft_pos48 *d_pos, const uint8_t *depths, uint32_t n,
                         uint64_t *d_out, void *stream);
+
+/* ------------------------------------------------------------- serving
+ * Continuous batching of perft queries (no counterpart in the reference,
+ * which runs one perft at a time from its CLI).  Queries of mixed depth are
+ * submitted at any time; admitted queries keep their frontier levels in
+ * HBM, and the levels of all in-flight queries with the same remaining
+ * depth are advanced together, a bounded number of items per scheduler
+ * iteration.  A query is admitted when its predicted level-buffer memory
+ * fits the budget.  Counts are identical to perft(). */
+typedef struct perft_serve_config {
+    uint64_t memory_bytes;   /* budget for resident frontiers (0: 90% of the free arena) */
+    uint64_t step_items;     /* items a level may advance per iteration (0: 2^27) */
+    uint32_t max_in_flight;  /* admitted queries at once (0: 4096, at most 65536) */
+} perft_serve_config;
+
+typedef struct perft_serve_stats {
+    uint64_t submitted, completed, in_flight, queued;
+    uint64_t iterations, launches;
+    uint64_t memory_budget, memory_reserved, memory_peak;
+    int      last_error;
+} perft_serve_stats;
+
+void perft_serve_config_default(perft_serve_config *cfg);
+int perft_serve_start(const perft_serve_config *cfg);   /* after perft_init */
+int perft_serve_stop(void);
+int perft_serve_submit(const perft_pos48 *pos, uint32_t depth, uint64_t *ticket);
+/* PERFT_OK with the count (and submit-to-completion latency) once done,
+ * PERFT_PENDING while running, PERFT_ERR_NOT_FOUND for unknown tickets.
+ * A completed ticket is consumed by the call that returns it. */
+int perft_serve_poll(uint64_t ticket, uint64_t *count, double *latency_s);
+int perft_serve_wait(uint64_t ticket, double timeout_s, uint64_t *count, double *latency_s);
+int perft_serve_get_stats(perft_serve_stats *out);
 
 /* ------------------------------------------------------- host utilities */
 

@@ -23,6 +23,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("PERFT_B200_LIB") or os.path.join(_HERE, "libperft_b200.so")
 
 PERFT_OK = 0
+PERFT_PENDING = 1
 PERFT_ERR_INVALID_ARG = -1
 PERFT_ERR_NOT_INITIALIZED = -2
 PERFT_ERR_CUDA = -3
@@ -90,6 +91,20 @@ class PerftStats(ctypes.Structure):
     ]
 
 
+class ServeConfig(ctypes.Structure):
+    _fields_ = [
+        ("memory_bytes", ctypes.c_uint64),
+        ("step_items", ctypes.c_uint64),
+        ("max_in_flight", ctypes.c_uint32),
+    ]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "submitted", "completed", "in_flight", "queued", "iterations", "launches",
+        "memory_budget", "memory_reserved", "memory_peak")] + [("last_error", ctypes.c_int)]
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -120,6 +135,14 @@ def _load():
         "perft_get_stats": (ctypes.c_int, [P(PerftStats)]),
         "perft_reset_stats": (ctypes.c_int, []),
         "perft_tt_clear": (ctypes.c_int, []),
+        "perft_serve_config_default": (None, [P(ServeConfig)]),
+        "perft_serve_start": (ctypes.c_int, [P(ServeConfig)]),
+        "perft_serve_stop": (ctypes.c_int, []),
+        "perft_serve_submit": (ctypes.c_int, [P(_Pos48), ctypes.c_uint32, P(ctypes.c_uint64)]),
+        "perft_serve_poll": (ctypes.c_int, [ctypes.c_uint64, P(ctypes.c_uint64), P(ctypes.c_double)]),
+        "perft_serve_wait": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_double, P(ctypes.c_uint64),
+                                            P(ctypes.c_double)]),
+        "perft_serve_get_stats": (ctypes.c_int, [P(ServeStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -238,6 +261,53 @@ def reset_stats() -> None:
 
 def tt_clear() -> None:
     _check(lib().perft_tt_clear(), "perft_tt_clear")
+
+
+# ---------------------------------------------------------------- serving
+def serve_start(memory_bytes: int = 0, step_items: int = 0, max_in_flight: int = 0) -> None:
+    """Starts the continuous-batching server (after init)."""
+    cfg = ServeConfig()
+    lib().perft_serve_config_default(ctypes.byref(cfg))
+    if memory_bytes:
+        cfg.memory_bytes = memory_bytes
+    if step_items:
+        cfg.step_items = step_items
+    if max_in_flight:
+        cfg.max_in_flight = max_in_flight
+    _check(lib().perft_serve_start(ctypes.byref(cfg)), "perft_serve_start")
+
+
+def serve_stop() -> None:
+    _check(lib().perft_serve_stop(), "perft_serve_stop")
+
+
+def serve_submit(pos, depth: int) -> int:
+    t = ctypes.c_uint64(0)
+    p = _pos(pos)
+    _check(lib().perft_serve_submit(ctypes.byref(p), int(depth), ctypes.byref(t)), "perft_serve_submit")
+    return int(t.value)
+
+
+def serve_poll(ticket: int):
+    """(count, latency_s) when done, None while the query runs."""
+    c, lat = ctypes.c_uint64(0), ctypes.c_double(0)
+    rc = lib().perft_serve_poll(ticket, ctypes.byref(c), ctypes.byref(lat))
+    if rc == PERFT_PENDING:
+        return None
+    _check(rc, "perft_serve_poll")
+    return int(c.value), float(lat.value)
+
+
+def serve_wait(ticket: int, timeout_s: float = 600.0):
+    c, lat = ctypes.c_uint64(0), ctypes.c_double(0)
+    _check(lib().perft_serve_wait(ticket, timeout_s, ctypes.byref(c), ctypes.byref(lat)), "perft_serve_wait")
+    return int(c.value), float(lat.value)
+
+
+def serve_stats() -> dict:
+    s = ServeStats()
+    _check(lib().perft_serve_get_stats(ctypes.byref(s)), "perft_serve_get_stats")
+    return {name: getattr(s, name) for name, _ in ServeStats._fields_}
 
 
 # ------------------------------------------------------- host utilities

@@ -13,7 +13,7 @@ LIB = os.path.join(HERE, "libperft_b200.so")
 PROBE_LIB = os.path.join(HERE, "libperft_probe.so")
 
 SOURCES = ["engine.cu", "tables.cpp", "host.cpp"]
-HEADERS = ["movegen.cuh", os.path.join("..", "..", "include", "perft_b200.h")]
+HEADERS = ["movegen.cuh", "serve.cuh", os.path.join("..", "..", "include", "perft_b200.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

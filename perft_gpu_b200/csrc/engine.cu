@@ -248,6 +248,8 @@ struct TileParams {
     // last ply output
     unsigned long long *rootCounts;
     u32 *err;
+    // serving: pending-node counter of each query slot (TRACK kernels only)
+    unsigned long long *pending;
 };
 
 // Emits a parent's moves, keeping only those whose global item index falls
@@ -263,10 +265,16 @@ struct WindowSink {
     }
 };
 
-template <int MODE, int SV>
+// TRACK (serving): besides the counts, every root run also accumulates the
+// change of its query's pending-node counter: +1 per child written, -1 when
+// a parent's last item is processed.  The counter reaching zero means the
+// query's subtree is fully counted.
+template <int MODE, int SV, bool TRACK = false>
 __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams P)
 {
     __shared__ u64 sb[6][TILE_MAXP];
+    __shared__ u64 sqEnd[TRACK ? TILE_MAXP : 1];
+    __shared__ int sdelta[TRACK ? TILE_MAXP : 1];
     __shared__ u32 sroot[TILE_MAXP];
     __shared__ u32 srun[TILE_MAXP];
     __shared__ u32 srunRoot[TILE_MAXP];
@@ -300,6 +308,7 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams P)
             const int nP = __syncthreads_count(valid);
             if (valid) {
                 qEnd = P.pscan[q + 1];
+                if (TRACK) sqEnd[tid] = qEnd;
 #pragma unroll
                 for (int k = 0; k < 6; k++) sb[k][tid] = P.ppl[k * P.pstride + q];
                 sroot[tid] = P.proot ? P.proot[q] : (u32)q;  // no root array: account to the parent itself
@@ -309,7 +318,7 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams P)
             __syncthreads();
 
             int nRuns = 0;
-            if (MODE == MODE_LEAF) {
+            if (MODE == MODE_LEAF || TRACK) {
                 // parents are ordered by root: number the runs of equal roots
                 const bool head = valid && (tid == 0 || sroot[tid] != sroot[tid - 1]);
                 const int r = block_excl_count<TILE_NT>(head, swarp, nRuns);
@@ -317,6 +326,7 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams P)
                 if (head) {
                     srunRoot[r] = sroot[tid];
                     sacc[r] = 0ull;
+                    if (TRACK) sdelta[r] = 0;
                 }
             }
 
@@ -360,15 +370,25 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams P)
                         pl = 0;
                     }
                 }
-                if (MODE == MODE_LEAF) {
+                if (MODE == MODE_LEAF || TRACK) {
                     const u32 key = act ? srun[pl] : 0xFFFFFFFFu;
                     const unsigned peers = __match_any_sync(0xffffffffu, key);
-                    const u32 sum = __reduce_add_sync(peers, cnt);
-                    if (act && lane == __ffs(peers) - 1) atomicAdd(&sacc[key], (unsigned long long)sum);
+                    if (MODE == MODE_LEAF) {
+                        const u32 sum = __reduce_add_sync(peers, cnt);
+                        if (act && lane == __ffs(peers) - 1) atomicAdd(&sacc[key], (unsigned long long)sum);
+                    }
+                    if (TRACK) {
+                        const bool lastOfParent = act && (sBeg + (u64)j + 1 == sqEnd[pl]);
+                        const int d = (act && MODE == MODE_EXPAND ? 1 : 0) - (lastOfParent ? 1 : 0);
+                        const int dsum = __reduce_add_sync(peers, d);
+                        if (act && lane == __ffs(peers) - 1 && dsum) atomicAdd(&sdelta[key], dsum);
+                    }
                 }
             }
             __syncthreads();
             if (MODE == MODE_LEAF && tid < nRuns) atomicAdd(&P.rootCounts[srunRoot[tid]], sacc[tid]);
+            if (TRACK && tid < nRuns && sdelta[tid])
+                atomicAdd(&P.pending[srunRoot[tid]], (unsigned long long)(long long)sdelta[tid]);
             if (sEnd >= iEnd || p + nP >= P.nParents) break;
             p += nP;
             __syncthreads();
@@ -616,6 +636,19 @@ private:
     bool alloc_level_tt(DeviceLevel &L, u64 n);
 
 public:
+    // A long-lived block at the top of the arena (the server's memory);
+    // per-call allocations stack above it.
+    char *reserve_block(u64 bytes)
+    {
+        blockMark = arenaTop;
+        char *p = (char *)alloc(bytes);
+        if (!p) arenaTop = blockMark;
+        return p;
+    }
+    void release_block() { arenaTop = blockMark; }
+    u64 free_bytes() const { return arena_free(); }
+    int device_id() const { return device; }
+    u64 blockMark = 0;
     int tt_clear();
     void read_tt_stats()
     {
@@ -1136,6 +1169,8 @@ Engine g_engine;
 
 }  // namespace
 
+#include "serve.cuh"
+
 namespace pg {
 // Shared with host.cpp: run a batch on the process-wide engine (host buffers).
 int engine_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *out);
@@ -1186,6 +1221,7 @@ int perft_init(const perft_config *cfg)
     perft_config c;
     if (cfg) c = *cfg;
     else perft_config_default(&c);
+    if (g_server.running) perft_serve_stop();
     std::lock_guard<std::mutex> lk(g_engine.mu);
     if (g_engine.ready) g_engine.shutdown();
     return g_engine.init(c);
@@ -1193,8 +1229,70 @@ int perft_init(const perft_config *cfg)
 
 int perft_shutdown(void)
 {
+    if (g_server.running) perft_serve_stop();
     std::lock_guard<std::mutex> lk(g_engine.mu);
     g_engine.shutdown();
+    return PERFT_OK;
+}
+
+void perft_serve_config_default(perft_serve_config *cfg)
+{
+    if (!cfg) return;
+    memset(cfg, 0, sizeof *cfg);
+    cfg->memory_bytes = 0;
+    cfg->step_items = 1ull << 27;
+    cfg->max_in_flight = 4096;
+}
+
+int perft_serve_start(const perft_serve_config *cfg)
+{
+    perft_serve_config c;
+    if (cfg) c = *cfg;
+    else perft_serve_config_default(&c);
+    std::lock_guard<std::mutex> lk(g_engine.mu);
+    if (!g_engine.ready) return PERFT_ERR_NOT_INITIALIZED;
+    if (g_server.running) return PERFT_ERR_INVALID_ARG;
+    const u64 fixed = 256ull << 20;  // slot tables, staging, scratch
+    u64 bytes = c.memory_bytes ? c.memory_bytes + fixed : (u64)(g_engine.free_bytes() * 0.9);
+    if (bytes > g_engine.free_bytes()) return PERFT_ERR_OUT_OF_MEMORY;
+    char *block = g_engine.reserve_block(bytes);
+    if (!block) return PERFT_ERR_OUT_OF_MEMORY;
+    const int rc = g_server.start(c, block, bytes, g_engine.device_id());
+    if (rc != PERFT_OK) g_engine.release_block();
+    return rc;
+}
+
+int perft_serve_stop(void)
+{
+    const bool was = g_server.running;
+    const int rc = g_server.stop();
+    std::lock_guard<std::mutex> lk(g_engine.mu);
+    if (was && g_engine.ready) g_engine.release_block();
+    return rc;
+}
+
+int perft_serve_submit(const perft_pos48 *pos, uint32_t depth, uint64_t *ticket)
+{
+    if (!pos || !ticket) return PERFT_ERR_INVALID_ARG;
+    if (!g_server.running) return PERFT_ERR_NOT_INITIALIZED;
+    return g_server.submit(pos->bb, depth, ticket);
+}
+
+int perft_serve_poll(uint64_t ticket, uint64_t *count, double *latency_s)
+{
+    return g_server.poll(ticket, count, latency_s, false, 0.0);
+}
+
+int perft_serve_wait(uint64_t ticket, double timeout_s, uint64_t *count, double *latency_s)
+{
+    return g_server.poll(ticket, count, latency_s, true, timeout_s);
+}
+
+int perft_serve_get_stats(perft_serve_stats *out)
+{
+    if (!out) return PERFT_ERR_INVALID_ARG;
+    memset(out, 0, sizeof *out);
+    g_server.get_stats(out);
     return PERFT_OK;
 }
 
