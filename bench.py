@@ -240,8 +240,17 @@ def run_ours(args):
     d_pos = torch.from_numpy(pos.view(np.int64)).cuda()
     d_out = torch.zeros(n, dtype=torch.int64, device="cuda")
 
-    def step_device():
-        pg.perft_batch_device(d_pos.data_ptr(), depths, n, d_out.data_ptr())
+    if args.form == "single":
+        # one position per call: the plain one-position-per-launch form
+        elem = d_pos.element_size() * 6
+
+        def step_device():
+            for i in range(n):
+                pg.perft_batch_device(d_pos.data_ptr() + i * elem, depths[i:i + 1], 1,
+                                      d_out.data_ptr() + i * d_out.element_size())
+    else:
+        def step_device():
+            pg.perft_batch_device(d_pos.data_ptr(), depths, n, d_out.data_ptr())
 
     for _ in range(args.warmup):
         step_device()
@@ -327,7 +336,8 @@ def run_ours(args):
         cpu = cpu_sample(pos, depths, args.cpu_seconds, expected=counts)
 
     cfg = dict(cfg)
-    cfg.update({"sliders": {"leaf": pg.SLIDER_NAMES.get(st["sliders_leaf"], "?"),
+    cfg.update({"form": "one perft call per position" if args.form == "single" else "one batched call",
+                "sliders": {"leaf": pg.SLIDER_NAMES.get(st["sliders_leaf"], "?"),
                             "interior": pg.SLIDER_NAMES.get(st["sliders_expand"], "?"),
                             "chosen_by": args.sliders},
                 "l2": "no flush: each step streams multi-GB level buffers through HBM (>> 126 MB L2)",
@@ -350,22 +360,115 @@ def run_ours(args):
     return 0
 
 
+def run_tt(args):
+    """Transposition-table workload: 4 seeded playouts of 12-24 plies at
+    depths 9-10 with a 2^30-entry table; parity with the no-table engine is
+    checked at depth 8 first."""
+    import perft_gpu_b200 as pg
+    from perft_gpu_b200 import workloads as W
+    pos, depths = W.tt_positions()
+    depths = np.minimum(depths, args.max_depth).astype(np.uint8)
+    pg.init(device=0)
+    t0 = time.perf_counter()
+    d8_plain = pg.perft_batch(pos, 8)
+    t_plain = time.perf_counter() - t0
+    pg.init(device=0, tt_log2_entries=args.tt_log2)
+    t0 = time.perf_counter()
+    d8_tt = pg.perft_batch(pos, 8)
+    t_tt8 = time.perf_counter() - t0
+    times, counts = [], None
+    for step in range(args.warmup + args.steps):
+        pg.tt_clear()
+        pg.reset_stats()
+        t0 = time.perf_counter()
+        counts = pg.perft_batch(pos, depths)
+        el = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(el)
+    st = pg.stats()
+    leaves = int(counts.sum())
+    line = {"metric": "perft leaf nodes/s with transposition table (effective, bit-exact)",
+            "value": leaves / float(np.mean(times)), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True,
+            "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "4 seeded playouts of 12-24 plies, TT of 2^%d x 16 B, table cleared each step"
+                                   % args.tt_log2, "depths": depths.tolist()},
+            "counts": [int(x) for x in counts],
+            "parity_depth8": {"equal": bool(np.array_equal(d8_plain, d8_tt)), "no_tt_s": t_plain, "tt_s": t_tt8,
+                              "counts": [int(x) for x in d8_plain]},
+            "tt": {k: st[k] for k in ("tt_entries", "tt_probes", "tt_hits", "tt_duplicates", "tt_stores")},
+            "timing": "host wall clock around the synchronous perft_batch call"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve(args):
+    """Serving workload: Poisson arrivals of seeded 0-40-ply positions at
+    depth U[3,7] through the continuous-batching server; p50/p99 latency is
+    submit-to-completion wall time."""
+    import perft_gpu_b200 as pg
+    from perft_gpu_b200 import workloads as W
+    pos, depths, arrivals = W.serving_trace(n=args.queries, rate_qps=args.rate, seed=5)
+    pg.init(device=0)
+    pg.serve_start(memory_bytes=int(args.serve_memory_gb * (1 << 30)))
+    tickets = [None] * len(pos)
+    t_start = time.perf_counter()
+    for i in range(len(pos)):
+        delay = t_start + arrivals[i] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        tickets[i] = pg.serve_submit(pos[i], int(depths[i]))
+    lat, counts = np.zeros(len(pos)), np.zeros(len(pos), dtype=np.uint64)
+    for i, t in enumerate(tickets):
+        c, l = pg.serve_wait(t, timeout_s=3600)
+        counts[i], lat[i] = c, l
+    wall = time.perf_counter() - t_start
+    st = pg.serve_stats()
+    pg.serve_stop()
+    # identity: a seeded sample of the queries, recomputed alone
+    sample = np.random.default_rng(1).choice(len(pos), min(256, len(pos)), replace=False)
+    alone = pg.perft_batch(pos[sample], depths[sample])
+    line = {"metric": "serving queries/s with p50/p99 latency", "value": len(pos) / wall, "unit": "queries/s",
+            "n_gpus": 1, "higher_is_better": True, "data": "synthetic", "dtype": "u64",
+            "config": {"workload": "Poisson arrivals, seeded 0-40-ply positions, depth U[3,7]",
+                       "offered_rate_qps": args.rate, "queries": len(pos),
+                       "memory_budget_gb": args.serve_memory_gb or "90% of free arena"},
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(lat.max())},
+            "leaf_nodes_per_s": float(counts.sum()) / wall,
+            "identical_alone_vs_mix": bool(np.array_equal(alone, counts[sample])),
+            "server": {k: st[k] for k in ("iterations", "launches", "memory_peak")}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batch", "start", "deep"], default="batch")
+    ap.add_argument("--workload", choices=["batch", "start", "deep", "tt", "serve"], default="batch")
     ap.add_argument("--sliders", choices=["auto", "kogge", "magic", "kogge_fma", "kogge_split"], default="auto")
     ap.add_argument("--positions", type=int, default=4096,
                     help="batch workload: use the first N positions (profiling runs)")
     ap.add_argument("--arena-gb", type=float, default=0.0, help="level-buffer arena (0 = 85%% of free HBM)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--form", choices=["batch", "single"], default="batch",
+                    help="batch workload: one batched call, or one call per position")
+    ap.add_argument("--tt-log2", type=int, default=30, help="tt workload: table entries (log2)")
+    ap.add_argument("--max-depth", type=int, default=10, help="tt workload: cap on the depths")
+    ap.add_argument("--rate", type=float, default=1000.0, help="serve workload: offered queries/s")
+    ap.add_argument("--queries", type=int, default=2000, help="serve workload: trace length")
+    ap.add_argument("--serve-memory-gb", type=float, default=120.0, help="serve workload: admission budget")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "tt":
+        return run_tt(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 
