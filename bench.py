@@ -115,13 +115,17 @@ def int32_peak(device):
             "imad_hi": out[5], "imad_wide_lop3": out[6]}
 
 
-def traffic_from_profiles(workload):
+def traffic_from_profiles(workload, items_per_launch):
+    """DRAM bytes per leaf launch: the ncu-measured bytes per item of a
+    captured launch (profiles/leaf_kernel_traffic.json) scaled to this run's
+    items per launch (traffic grows with the items processed)."""
     path = os.path.join(ROOT, "profiles", "leaf_kernel_traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
         d = json.load(f)
-    return d.get(workload, {}).get("dram_bytes_per_launch")
+    per_item = d.get(workload, {}).get("dram_bytes_per_item")
+    return per_item * items_per_launch if per_item is not None else None
 
 
 # ------------------------------------------------------------------ workloads
@@ -324,7 +328,8 @@ def run_ours(args):
         "frac": (achieved / peak) if (achieved and peak) else None,
         "peak_source": "of measured: best of the integer instruction mixes timed on this GPU by libperft_probe.so",
         "peak_variants_tops": {k: v / 1e12 for k, v in peaks.items()} if peaks else None,
-        "traffic": traffic_from_profiles(wf_key),
+        "traffic": traffic_from_profiles(wf_key, st["leaf_items"] / launches),
+        "traffic_unit": "bytes per leaf launch (ncu bytes/item x items/launch)",
         "work_per_launch_ops": w_int / launches,
         "leaf_launch_ms_avg": st["leaf_ms"] / launches,
         "leaf_share_of_step": (st["leaf_ms"] / ms) if ms > 0 else None,
