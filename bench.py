@@ -454,7 +454,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["batch", "start", "deep", "tt", "serve"], default="batch")
-    ap.add_argument("--sliders", choices=["auto", "kogge", "magic", "kogge_fma", "kogge_split"], default="auto")
+    ap.add_argument("--sliders", choices=["auto", "kogge", "magic", "kogge_fma", "kogge_split", "hybrid"], default="auto")
     ap.add_argument("--positions", type=int, default=4096,
                     help="batch workload: use the first N positions (profiling runs)")
     ap.add_argument("--arena-gb", type=float, default=0.0, help="level-buffer arena (0 = 85%% of free HBM)")

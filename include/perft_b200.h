@@ -58,6 +58,7 @@ typedef struct perft_pos48 {
 #define PERFT_SLIDERS_MAGIC      1  /* fancy magic lookups */
 #define PERFT_SLIDERS_KOGGE_FMA  2  /* Kogge-Stone, constant shifts on the FMA pipe */
 #define PERFT_SLIDERS_KOGGE_SPLIT 3 /* Kogge-Stone, left shifts split over ALU and FMA pipes */
+#define PERFT_SLIDERS_HYBRID      4 /* attack map by fills, own slider moves by magic lookups */
 
 typedef struct perft_config {
     int      device;          /* CUDA device ordinal */

@@ -40,8 +40,9 @@ SLIDERS_KOGGE = 0
 SLIDERS_MAGIC = 1
 SLIDERS_KOGGE_FMA = 2
 SLIDERS_KOGGE_SPLIT = 3
+SLIDERS_HYBRID = 4
 SLIDER_NAMES = {SLIDERS_KOGGE: "kogge", SLIDERS_MAGIC: "magic", SLIDERS_KOGGE_FMA: "kogge_fma",
-                SLIDERS_KOGGE_SPLIT: "kogge_split"}
+                SLIDERS_KOGGE_SPLIT: "kogge_split", SLIDERS_HYBRID: "hybrid"}
 
 START_FEN = "rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1"
 

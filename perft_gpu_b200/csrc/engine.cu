@@ -714,6 +714,7 @@ void launch_tile_variant(int sv, int grid, cudaStream_t st, const TileParams &P)
     case SV_MAGIC: k_tile<MODE, SV_MAGIC><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P); break;
     case SV_KOGGE_FMA: k_tile<MODE, SV_KOGGE_FMA><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P); break;
     case SV_KOGGE_SPLIT: k_tile<MODE, SV_KOGGE_SPLIT><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P); break;
+    case SV_HYBRID: k_tile<MODE, SV_HYBRID><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P); break;
     default: k_tile<MODE, SV_KOGGE><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P); break;
     }
 }
@@ -725,6 +726,7 @@ const char *slider_name(int sv)
     case SV_MAGIC: return "magic";
     case SV_KOGGE_FMA: return "kogge_fma";
     case SV_KOGGE_SPLIT: return "kogge_split";
+    case SV_HYBRID: return "hybrid";
     default: return "?";
     }
 }
@@ -795,6 +797,8 @@ int Engine::init(const perft_config &cfg)
     gridTile[MODE_LEAF][SV_MAGIC] = occupancy_grid<MODE_LEAF, SV_MAGIC>(nsm);
     gridTile[MODE_LEAF][SV_KOGGE_FMA] = occupancy_grid<MODE_LEAF, SV_KOGGE_FMA>(nsm);
     gridTile[MODE_LEAF][SV_KOGGE_SPLIT] = occupancy_grid<MODE_LEAF, SV_KOGGE_SPLIT>(nsm);
+    gridTile[MODE_EXPAND][SV_HYBRID] = occupancy_grid<MODE_EXPAND, SV_HYBRID>(nsm);
+    gridTile[MODE_LEAF][SV_HYBRID] = occupancy_grid<MODE_LEAF, SV_HYBRID>(nsm);
 
     auto pick = [](int v) { return (v >= 0 && v < SV_COUNT) ? v : SV_KOGGE; };
     svExpand = pick(cfg.sliders_expand);

@@ -34,6 +34,14 @@
 
 // Knight moves of the Kogge-Stone variants: 0 = eight jump shifts over the
 // whole knight set, 1 = one table lookup per knight.
+// PG_FUSED_COUNT 1: Kogge-Stone counts use count_moves_fused.
+#ifndef PG_FUSED_COUNT
+#define PG_FUSED_COUNT 1
+#endif
+// PG_RANK_SUB 1: east/west rays of the fused count by carry subtraction.
+#ifndef PG_RANK_SUB
+#define PG_RANK_SUB 1
+#endif
 #ifndef PG_KNIGHT_LUT
 #define PG_KNIGHT_LUT 1
 #endif
@@ -82,7 +90,8 @@ enum SliderVariant : int {
     SV_MAGIC = 1,      // fancy magic lookups, one per piece
     SV_KOGGE_FMA = 2,  // occluded fills with every constant shift on the FMA pipe
     SV_KOGGE_SPLIT = 3,  // left shifts split: high word on the ALU, low word on the FMA pipe
-    SV_COUNT = 4,
+    SV_HYBRID = 4,       // opponent attack map by split-shift fills, own slider moves by magic lookups
+    SV_COUNT = 5,
 };
 
 // How a Kogge-Stone fill issues its constant shifts.
@@ -92,7 +101,9 @@ enum ShiftMode : int { SH_ALU = 0, SH_FMA = 1, SH_SPLIT = 2 };
 template <int SV>
 struct SvTraits {
     static constexpr bool kogge = SV != SV_MAGIC;
-    static constexpr int shift = SV == SV_KOGGE_FMA ? SH_FMA : (SV == SV_KOGGE_SPLIT ? SH_SPLIT : SH_ALU);
+    static constexpr bool ownMagic = SV == SV_HYBRID;  // own slider moves by lookups
+    static constexpr int shift =
+        SV == SV_KOGGE_FMA ? SH_FMA : ((SV == SV_KOGGE_SPLIT || SV == SV_HYBRID) ? SH_SPLIT : SH_ALU);
 };
 
 // ------------------------------------------------------------------ tables
@@ -462,10 +473,233 @@ PG_HD u64 check_mask(const Ctx &c)
     return chk | PG_TAB(between[c.ksq][ctz(chk)]);
 }
 
+// One Kogge-Stone direction for two generator sets sharing one propagator
+// chain (built from the empty squares): the opponent's sliders add to the
+// attack map, this side's unpinned sliders add their move count.
+template <int S, bool LEFT, int MODE>
+PG_HD void ks_pair(u64 eGen, u64 oGen, u64 empty, u64 wrap, u64 targets, u64 &attacked, u32 &n)
+{
+    const u64 p0 = empty & wrap;
+    u64 e = eGen, o = oGen;
+    if (LEFT) {
+        const u64 p1 = p0 & shl<S, MODE>(p0);
+        const u64 p2 = p1 & shl<2 * S, MODE>(p1);
+        e |= p0 & shl<S, MODE>(e);
+        o |= p0 & shl<S, MODE>(o);
+        e |= p1 & shl<2 * S, MODE>(e);
+        o |= p1 & shl<2 * S, MODE>(o);
+        e |= p2 & shl<4 * S, MODE>(e);
+        o |= p2 & shl<4 * S, MODE>(o);
+        attacked |= shl<S, MODE>(e) & wrap;
+        n += popc(shl<S, MODE>(o) & wrap & targets);
+    } else {
+        const u64 p1 = p0 & shr<S, MODE>(p0);
+        const u64 p2 = p1 & shr<2 * S, MODE>(p1);
+        e |= p0 & shr<S, MODE>(e);
+        o |= p0 & shr<S, MODE>(o);
+        e |= p1 & shr<2 * S, MODE>(e);
+        o |= p1 & shr<2 * S, MODE>(o);
+        e |= p2 & shr<4 * S, MODE>(e);
+        o |= p2 & shr<4 * S, MODE>(o);
+        attacked |= shr<S, MODE>(e) & wrap;
+        n += popc(shr<S, MODE>(o) & wrap & targets);
+    }
+}
+
+// 64-bit bit reversal (file h <-> a, rank 8 <-> 1 mirrored together).
+PG_HD u64 brev64(u64 x)
+{
+#ifdef __CUDA_ARCH__
+    return __brevll(x);
+#else
+    x = ((x >> 1) & 0x5555555555555555ULL) | ((x & 0x5555555555555555ULL) << 1);
+    x = ((x >> 2) & 0x3333333333333333ULL) | ((x & 0x3333333333333333ULL) << 2);
+    x = ((x >> 4) & 0x0F0F0F0F0F0F0F0FULL) | ((x & 0x0F0F0F0F0F0F0F0FULL) << 4);
+    return __builtin_bswap64(x);
+#endif
+}
+
+// East attacks of a slider set by carry subtraction.  `os` is the occupancy
+// with a sentinel on every a-file square: subtracting 2g from it borrows
+// through the empty squares east of each slider g and stops at (and clears)
+// the first occupied square or the next rank's sentinel, so os ^ (os - 2G)
+// marks exactly the squares each slider reaches, blocker included, plus
+// sentinels that the a-file mask removes.  Borrow chains of different
+// sliders never overlap: a chain stops at or before the next slider east
+// on its rank, and each subtraction starts just east of its slider.
+PG_HD u64 east_sub(u64 G, u64 os)
+{
+    return (os ^ (os - (G + G))) & ~FILEA;
+}
+
+// One rank direction pair: the opponent's fill feeds the attack map, this
+// side's fill is counted.  WEST mirrors the board with bit reversal.
+template <bool WEST>
+PG_HD void rank_pair(u64 eGen, u64 oGen, u64 os, u64 targets, u64 &attacked, u32 &n)
+{
+    if (!WEST) {
+        attacked |= east_sub(eGen, os);
+        n += popc(east_sub(oGen, os) & targets);
+    } else {
+        attacked |= brev64(east_sub(brev64(eGen), os));
+        n += popc(brev64(east_sub(brev64(oGen), os)) & targets);
+    }
+}
+
+// countMoves for the Kogge-Stone variants, fused:
+//  * checkers come first, straight from the king square (pawn, knight and
+//    two slider lookups), so the check mask is known before any move count;
+//  * the opponent's attack map treats this side's king as opaque, which lets
+//    every direction build one propagator chain for both the opponent's
+//    fill and this side's fill; the only square an opaque king hides is the
+//    one behind it on a slider checker's line, which is added back (x-ray).
+template <int SV>
+PG_HD u32 count_moves_fused(const Board &b)
+{
+    constexpr int M = SvTraits<SV>::shift;
+    const u64 pawns = b.pawns & RANKS2TO7;
+    const u64 occ = pawns | b.knights | b.bq | b.rq | b.kings;
+    const u64 mine = b.mine, theirs = occ ^ mine, empty = ~occ, notMine = ~mine;
+    const u64 myK = b.kings & mine;
+    const int ksq = ctz(myK);
+    const u64 tP = pawns & theirs, tN = b.knights & theirs, tB = b.bq & theirs, tR = b.rq & theirs;
+    const u32 st = (u32)(b.pawns & 0xFF);
+
+    const u64 chk = (pawn_att_up(myK) & tP) | (PG_TAB(knight[ksq]) & tN) | (magic_bishop(ksq, occ) & tB) |
+                    (magic_rook(ksq, occ) & tR);
+    u64 cm = ~0ULL, xray = 0;
+    if (chk) {
+        cm = (chk & (chk - 1)) ? 0 : (chk | PG_TAB(between[ksq][ctz(chk)]));
+        u64 sl = chk & (tB | tR);
+        while (sl) {
+            const int c = ctz(sl);
+            sl &= sl - 1;
+            xray |= PG_TAB(line[ksq][c]) & ~PG_TAB(between[ksq][c]) & ~(1ULL << c);
+        }
+    }
+    const bool inCheck = chk != 0;
+
+    // pins: each pinned piece may only move along its pin line
+    u64 pinned = 0;
+    u32 nPinned = 0;
+    u64 snipers = (PG_TAB(rookRays[ksq]) & tR) | (PG_TAB(bishopRays[ksq]) & tB);
+    while (snipers) {
+        const int s = ctz(snipers);
+        snipers &= snipers - 1;
+        const u64 btw = PG_TAB(between[ksq][s]);
+        const u64 blk = btw & occ;
+        if (!blk || (blk & (blk - 1)) || !(blk & mine)) continue;
+        pinned |= blk;
+        const bool diag = (PG_TAB(bishopRays[ksq]) >> s) & 1;
+        if (blk & (diag ? b.bq : b.rq)) {
+            nPinned += popc(btw);
+        } else if (blk & pawns) {
+            if (diag) {
+                const u64 cap = pawn_att_up(blk) & (1ULL << s);
+                nPinned += popc(cap) + 3 * popc(cap & RANK8);
+            } else if (((ksq ^ s) & 7) == 0) {
+                const u64 p1 = sh_n(blk) & empty;
+                nPinned += popc(p1) + popc(sh_n(p1 & RANK3) & empty);
+            }
+        }
+    }
+    u32 n = inCheck ? 0 : nPinned;  // pinned pieces never resolve a check
+    const u64 targets = notMine & cm;
+
+    // sliders and the opponent's slider attacks, direction by direction
+    const u64 B = b.bq & mine & ~pinned, R = b.rq & mine & ~pinned;
+    u64 attacked = 0;
+    if (SvTraits<SV>::ownMagic) {
+        attacked = ks_orth<M>(tR, empty) | ks_diag<M>(tB, empty);
+        u64 x = B;
+        while (x) {
+            n += popc(magic_bishop(ctz(x), occ) & targets);
+            x &= x - 1;
+        }
+        x = R;
+        while (x) {
+            n += popc(magic_rook(ctz(x), occ) & targets);
+            x &= x - 1;
+        }
+    } else {
+        ks_pair<8, true, M>(tR, R, empty, ~0ULL, targets, attacked, n);
+        ks_pair<8, false, M>(tR, R, empty, ~0ULL, targets, attacked, n);
+        if (PG_RANK_SUB) {
+            rank_pair<false>(tR, R, occ | FILEA, targets, attacked, n);
+            rank_pair<true>(tR, R, brev64(occ) | FILEA, targets, attacked, n);
+        } else {
+            ks_pair<1, true, M>(tR, R, empty, ~FILEA, targets, attacked, n);
+            ks_pair<1, false, M>(tR, R, empty, ~FILEH, targets, attacked, n);
+        }
+        ks_pair<9, true, M>(tB, B, empty, ~FILEA, targets, attacked, n);
+        ks_pair<7, true, M>(tB, B, empty, ~FILEH, targets, attacked, n);
+        ks_pair<7, false, M>(tB, B, empty, ~FILEA, targets, attacked, n);
+        ks_pair<9, false, M>(tB, B, empty, ~FILEH, targets, attacked, n);
+    }
+    attacked |= pawn_att_down(tP) | knight_set_att(tN) | PG_TAB(king[ctz(b.kings & theirs)]);
+
+    // king
+    n += popc(PG_TAB(king[ksq]) & notMine & ~(attacked | xray));
+    if (!cm) return n;  // double check: king moves only
+
+    // castling (relative squares: king e1, rooks h1/a1), never out of check
+    if (!inCheck) {
+        if ((st & 1) && !((occ | attacked) & 0x60ULL)) n++;
+        if ((st & 2) && !(occ & 0x0EULL) && !(attacked & 0x0CULL)) n++;
+    }
+
+    // free pawns, set-wise
+    const u64 P = pawns & mine & ~pinned;
+    const u64 p1 = sh_n(P) & empty;
+    const u64 p1c = p1 & cm;
+    n += popc(p1c) + 3 * popc(p1c & RANK8);
+    n += popc(sh_n(p1 & RANK3) & empty & cm);
+    const u64 capT = theirs & cm;
+    const u64 cl = sh_nw(P) & capT, cr = sh_ne(P) & capT;
+    n += popc(cl) + popc(cr) + 3 * (popc(cl & RANK8) + popc(cr & RANK8));
+
+    // en passant: out of check, or capturing the checking pawn
+    const u32 epf = st >> 4;
+    if (epf) {
+        const u64 target = 1ULL << (39 + epf);
+        const u64 captured = sh_s(target);
+        if (!inCheck || (captured & cm)) {
+            u64 srcs = pawn_att_down(target) & pawns & mine;
+            while (srcs) {
+                const u64 sb = srcs & (0 - srcs);
+                srcs ^= sb;
+                if (sb & pinned) {
+                    if (!inCheck && (PG_TAB(line[ctz(sb)][ksq]) & target)) n++;
+                } else if (myK & RANK5) {
+                    const u64 pro = empty | sb | captured;
+                    if (!((ks_east(myK, pro) | ks_west(myK, pro)) & tR)) n++;
+                } else {
+                    n++;
+                }
+            }
+        }
+    }
+
+    // knights
+    u64 N = b.knights & mine & ~pinned;
+    if (PG_KNIGHT_LUT) {
+        while (N) {
+            n += popc(PG_TAB(knight[ctz(N)]) & targets);
+            N &= N - 1;
+        }
+    } else {
+        n += knight_set_count(N, targets);
+    }
+    return n;
+}
+
 // Legal move count of the side to move (countMoves).
 template <int SV>
 PG_HD u32 count_moves(const Board &b)
 {
+#if PG_FUSED_COUNT
+    if (SvTraits<SV>::kogge) return count_moves_fused<SV>(b);
+#endif
     Ctx c;
     setup_ctx<SV>(b, c);
     const u64 notMine = ~c.mine;

@@ -44,6 +44,7 @@ int hc_init(void)
 uint32_t hc_count(const uint64_t pos[6], int sv)
 {
     Board b = from_pos48(pos);
+    if (sv == 4) return count_moves<SV_HYBRID>(b);
     return sv ? count_moves<SV_MAGIC>(b) : count_moves<SV_KOGGE>(b);
 }
 
@@ -65,6 +66,7 @@ uint32_t hc_children(const uint64_t pos[6], int sv, uint64_t *out)
 uint64_t hc_perft(const uint64_t pos[6], uint32_t depth, int sv)
 {
     Board b = from_pos48(pos);
+    if (sv == 4) return perft_rel<SV_HYBRID>(b, depth);
     return sv ? perft_rel<SV_MAGIC>(b, depth) : perft_rel<SV_KOGGE>(b, depth);
 }
 

@@ -124,7 +124,7 @@ def test_divide_sums_to_perft(engine):
         assert sorted(div) == sorted(engine.legal_moves(p))
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3], ids=["kogge", "magic", "kogge_fma", "kogge_split"])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4], ids=["kogge", "magic", "kogge_fma", "kogge_split", "hybrid"])
 def test_slider_variants(engine, golden, oracle, variant):
     """Every slider variant, on interior and last plies alike, is bit-exact."""
     engine.init(device=0, arena_bytes=2 << 30, sliders_expand=variant, sliders_leaf=variant)

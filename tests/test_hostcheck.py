@@ -35,7 +35,7 @@ def _children(hc, pos, sv):
     return sorted(tuple(buf[6 * i:6 * i + 6]) for i in range(n))
 
 
-@pytest.mark.parametrize("sv", [0, 1], ids=["kogge", "magic"])
+@pytest.mark.parametrize("sv", [0, 1, 4], ids=["kogge", "magic", "hybrid"])
 def test_golden_perft(hc, golden, sv):
     for e in golden:
         p = P6(*[int(h, 16) for h in e["pos48"]])
