@@ -197,6 +197,7 @@ typedef struct perft_stats {
     uint64_t tt_hits;            /* lookups answered by the table */
     uint64_t tt_duplicates;      /* same-level transpositions expanded once */
     uint64_t tt_stores;          /* entries written */
+    uint64_t graph_launches;     /* batches run as one replayed device-driven graph */
 } perft_stats;
 
 int perft_get_stats(perft_stats *out);

@@ -89,6 +89,7 @@ class PerftStats(ctypes.Structure):
         ("tt_hits", ctypes.c_uint64),
         ("tt_duplicates", ctypes.c_uint64),
         ("tt_stores", ctypes.c_uint64),
+        ("graph_launches", ctypes.c_uint64),
     ]
 
 

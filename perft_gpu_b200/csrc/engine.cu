@@ -60,8 +60,10 @@ namespace {
 #define PG_TILE_MINB 3
 #endif
 constexpr int TILE_NT = 256;
-constexpr int TILE_CAP_LOG2 = PG_TILE_CAP_LOG2;  // items per tile = 2^TILE_CAP_LOG2
+constexpr int TILE_CAP_LOG2 = PG_TILE_CAP_LOG2;  // largest tile: 2^TILE_CAP_LOG2 items
 constexpr int TILE_CAP = 1 << TILE_CAP_LOG2;
+constexpr int TILE_MIN_LOG2 = 10;  // small levels use tiles down to 1024 items to fill every SM
+constexpr u64 MAX_TILES_PER_NODE_DIV = 1ull << TILE_MIN_LOG2;
 constexpr int TILE_MAXP = TILE_NT;
 constexpr int TILE_MINB = PG_TILE_MINB;          // resident CTAs per SM the register budget targets
 constexpr int MAX_LEGAL_MOVES = 218;
@@ -80,7 +82,7 @@ enum { MODE_EXPAND = 0, MODE_LEAF = 1 };
 // Bytes of one level node: 6 planes + count + root + scan entry, plus its
 // share of the tile index (4 B per TILE_CAP items, up to 218 items a node)
 // and of the scan's block sums, rounded up.
-constexpr u64 NODE_BYTES = 6 * 8 + 4 + 4 + 8 + 1;
+constexpr u64 NODE_BYTES = 6 * 8 + 4 + 4 + 8 + 1;  // (tile index sized for the smallest tile: < 1 B/node)
 
 // --------------------------------------------------------- block helpers
 template <int NT>
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(SCAN_TOP_NT) k_scan_top(u64 *__restrict__ bsum
 __global__ void __launch_bounds__(SCAN_NT) k_scan_apply(const u32 *__restrict__ cnt, u64 n,
                                                         const u64 *__restrict__ bsum,
                                                         u64 *__restrict__ scan,
-                                                        u32 *__restrict__ tileFirst)
+                                                        u32 *__restrict__ tileFirst, int capLog2)
 {
     __shared__ u32 s[SCAN_CHUNK];
     __shared__ u64 sw[SCAN_NT / 32];
@@ -190,8 +192,8 @@ __global__ void __launch_bounds__(SCAN_NT) k_scan_apply(const u32 *__restrict__ 
         const u32 c = s[threadIdx.x * SCAN_IPT + k];
         scan[idx] = run;
         if (c) {
-            const u64 t0 = (run + TILE_CAP - 1) >> TILE_CAP_LOG2;
-            const u64 t1 = (run + c - 1) >> TILE_CAP_LOG2;
+            const u64 t0 = (run + (1ull << capLog2) - 1) >> capLog2;
+            const u64 t1 = (run + c - 1) >> capLog2;
             for (u64 t = t0; t <= t1; t++) tileFirst[t] = (u32)idx;
         }
         run += c;
@@ -229,6 +231,142 @@ __global__ void k_init_roots(const u64 *__restrict__ pos48, const u32 *__restric
     if (depth == 1) rootCounts[id] = c;
 }
 
+// ------------------------------------------- device-driven level pipeline
+// The scan of level k runs with a fixed grid (grid-stride over chunks), its
+// top block computes the total and bump-allocates level k+1 and that
+// level's scan buffers from a device-resident plan.  No host round trip
+// separates the plies, so a whole perft is one captured CUDA graph.  If the
+// region is exhausted the plan's overflow flag is raised, every following
+// level is empty, and the host reruns the batch on the host-driven path.
+// A level whose sizes and buffers are decided on the device (device-driven
+// pipeline, no host round trip between plies).
+struct LevelDesc {
+    u64 *planes;
+    u64 stride;
+    u32 *cnt;
+    u32 *root;
+    u64 n;
+    u64 *pscan;
+    u32 *tileFirst;
+    u64 *bsum;
+    u64 total;
+    int capLog2;  // tile size of this level's items
+};
+
+constexpr int DD_MAX_LEVELS = 24;
+struct DevPlan {
+    char *base;
+    u64 cap;
+    u64 bump;
+    u32 overflow;
+    u32 tileTarget;  // smallest tile count a level should have (2 x resident CTAs)
+    LevelDesc lv[DD_MAX_LEVELS];
+};
+
+__device__ __forceinline__ void *dd_take(DevPlan *plan, u64 bytes)
+{
+    const u64 a = (plan->bump + 255) & ~255ULL;
+    if (a + bytes > plan->cap) {
+        plan->overflow = 1;
+        return nullptr;
+    }
+    plan->bump = a + bytes;
+    return plan->base + a;
+}
+
+__global__ void __launch_bounds__(SCAN_NT) k_dd_scan_reduce(DevPlan *plan, int lv)
+{
+    __shared__ u64 sw[SCAN_NT / 32];
+    const LevelDesc &L = plan->lv[lv];
+    const u64 n = L.n, nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    for (u64 b = blockIdx.x; b < nb; b += gridDim.x) {
+        const u64 base = b * SCAN_CHUNK;
+        u64 s = 0;
+        for (int i = threadIdx.x; i < SCAN_CHUNK; i += SCAN_NT) {
+            const u64 k = base + i;
+            if (k < n) s += L.cnt[k];
+        }
+        u64 total;
+        block_excl_scan_u64<SCAN_NT>(s, sw, total);
+        if (threadIdx.x == 0) L.bsum[b] = total;
+    }
+}
+
+__global__ void __launch_bounds__(SCAN_TOP_NT) k_dd_scan_top(DevPlan *plan, int lv, int last)
+{
+    __shared__ u64 sw[SCAN_TOP_NT / 32];
+    LevelDesc &L = plan->lv[lv];
+    const u64 n = L.n, nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    const u64 per = (nb + SCAN_TOP_NT - 1) / SCAN_TOP_NT;
+    const u64 b0 = per * threadIdx.x, b1 = min(b0 + per, nb);
+    u64 s = 0;
+    for (u64 i = b0; i < b1; i++) s += L.bsum[i];
+    u64 total;
+    u64 run = block_excl_scan_u64<SCAN_TOP_NT>(s, sw, total);
+    for (u64 i = b0; i < b1; i++) {
+        const u64 v = L.bsum[i];
+        L.bsum[i] = run;
+        run += v;
+    }
+    if (threadIdx.x != 0) return;
+    if (n) L.pscan[n] = total;
+    L.total = plan->overflow ? 0 : total;
+    int cap = TILE_CAP_LOG2;
+    while (cap > TILE_MIN_LOG2 && (total >> cap) < plan->tileTarget) cap--;
+    L.capLog2 = cap;
+    if (last) return;
+    LevelDesc &C = plan->lv[lv + 1];
+    const u64 m = L.total;
+    C.n = m;
+    C.stride = (m + 31) & ~31ULL;
+    C.total = 0;
+    C.planes = (u64 *)dd_take(plan, 48 * C.stride);
+    C.cnt = (u32 *)dd_take(plan, 4 * C.stride);
+    C.root = (u32 *)dd_take(plan, 4 * C.stride);
+    C.pscan = (u64 *)dd_take(plan, 8 * (m + 1));
+    C.tileFirst = (u32 *)dd_take(plan, 4 * ((m * MAX_LEGAL_MOVES) / MAX_TILES_PER_NODE_DIV + 2));
+    C.bsum = (u64 *)dd_take(plan, 8 * ((m + SCAN_CHUNK - 1) / SCAN_CHUNK + 1));
+    if (plan->overflow) {
+        C.n = 0;
+        L.total = 0;  // nothing is expanded into a level that does not exist
+    }
+}
+
+__global__ void __launch_bounds__(SCAN_NT) k_dd_scan_apply(DevPlan *plan, int lv)
+{
+    __shared__ u32 s[SCAN_CHUNK];
+    __shared__ u64 sw[SCAN_NT / 32];
+    const LevelDesc &L = plan->lv[lv];
+    const u64 n = L.n, nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    for (u64 b = blockIdx.x; b < nb; b += gridDim.x) {
+        const u64 base = b * SCAN_CHUNK;
+        for (int i = threadIdx.x; i < SCAN_CHUNK; i += SCAN_NT) {
+            const u64 k = base + i;
+            s[i] = k < n ? L.cnt[k] : 0u;
+        }
+        __syncthreads();
+        u64 local = 0;
+#pragma unroll
+        for (int k = 0; k < SCAN_IPT; k++) local += s[threadIdx.x * SCAN_IPT + k];
+        u64 total;
+        u64 run = L.bsum[b] + block_excl_scan_u64<SCAN_NT>(local, sw, total);
+        for (int k = 0; k < SCAN_IPT; k++) {
+            const u64 idx = base + (u64)threadIdx.x * SCAN_IPT + k;
+            if (idx >= n) break;
+            const u32 c = s[threadIdx.x * SCAN_IPT + k];
+            L.pscan[idx] = run;
+            if (c) {
+                const int cl = L.capLog2;
+                const u64 t0 = (run + (1ull << cl) - 1) >> cl;
+                const u64 t1 = (run + c - 1) >> cl;
+                for (u64 t = t0; t <= t1; t++) L.tileFirst[t] = (u32)idx;
+            }
+            run += c;
+        }
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------ tile kernel
 struct TileParams {
     const u64 *ppl;   // parent planes, plane i at ppl + i * pstride
@@ -237,8 +375,9 @@ struct TileParams {
     const u32 *proot;  // root id of each parent; null: sums go to the parent's own slot
     u64 nParents;
     const u32 *tileFirst;  // indexed by absolute tile number
-    u64 itemBase;     // first item of this launch (multiple of TILE_CAP)
+    u64 itemBase;     // first item of this launch (multiple of the tile size)
     u64 itemEnd;      // one past the last item
+    int capLog2;      // tile size of this level (the scan's tileFirst granularity)
     u32 *tileCounter; // work-stealing cursor, zeroed before launch
     // interior ply outputs (child index = item - itemBase)
     u64 *cpl;
@@ -250,7 +389,12 @@ struct TileParams {
     u32 *err;
     // serving: pending-node counter of each query slot (TRACK kernels only)
     unsigned long long *pending;
+    // device-driven runs (DD kernels only): parent/child level descriptors
+    // written on the device by the previous scan; they override the fields above
+    const struct LevelDesc *dpar;
+    const struct LevelDesc *dch;
 };
+
 
 // Emits a parent's moves, keeping only those whose global item index falls
 // inside [lo, hi): the window of the current tile.
@@ -269,9 +413,29 @@ struct WindowSink {
 // change of its query's pending-node counter: +1 per child written, -1 when
 // a parent's last item is processed.  The counter reaching zero means the
 // query's subtree is fully counted.
-template <int MODE, int SV, bool TRACK = false>
-__global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams P)
+template <int MODE, int SV, bool TRACK = false, bool DD = false>
+__global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pin)
 {
+    TileParams P = Pin;
+    if (DD) {
+        const LevelDesc &a = *Pin.dpar;
+        P.ppl = a.planes;
+        P.pstride = a.stride;
+        P.pscan = a.pscan;
+        P.proot = a.root;
+        P.nParents = a.n;
+        P.tileFirst = a.tileFirst;
+        P.itemBase = 0;
+        P.itemEnd = a.total;
+        P.capLog2 = a.capLog2;
+        if (MODE == MODE_EXPAND) {
+            const LevelDesc &c = *Pin.dch;
+            P.cpl = c.planes;
+            P.cstride = c.stride;
+            P.ccnt = c.cnt;
+            P.croot = c.root;
+        }
+    }
     __shared__ u64 sb[6][TILE_MAXP];
     __shared__ u64 sqEnd[TRACK ? TILE_MAXP : 1];
     __shared__ int sdelta[TRACK ? TILE_MAXP : 1];
@@ -284,16 +448,17 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams P)
     __shared__ u32 sTile;
 
     const int tid = threadIdx.x, lane = tid & 31;
-    const u64 tile0 = P.itemBase >> TILE_CAP_LOG2;
-    const u64 nTiles = (P.itemEnd - P.itemBase + TILE_CAP - 1) >> TILE_CAP_LOG2;
+    const int capLog2 = P.capLog2;
+    const u64 tile0 = P.itemBase >> capLog2;
+    const u64 nTiles = (P.itemEnd - P.itemBase + (1ull << capLog2) - 1) >> capLog2;
 
     for (;;) {
         if (tid == 0) sTile = atomicAdd(P.tileCounter, 1u);
         __syncthreads();
         const u64 tl = sTile;
         if (tl >= nTiles) break;
-        const u64 iBeg = P.itemBase + (tl << TILE_CAP_LOG2);
-        const u64 iEnd = min(iBeg + (u64)TILE_CAP, P.itemEnd);
+        const u64 iBeg = P.itemBase + (tl << capLog2);
+        const u64 iEnd = min(iBeg + ((u64)1 << capLog2), P.itemEnd);
         u64 p = P.tileFirst[tile0 + tl];
 
         for (;;) {
@@ -597,6 +762,12 @@ public:
     int init(const perft_config &cfg);
     void shutdown();
     int run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut);
+    // Host buffers: staged through engine-owned device buffers that persist
+    // across calls (no per-call allocation; stable addresses let replayed
+    // graphs be reused).
+    int run_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *out);
+    u64 *ioPos = nullptr, *ioOut = nullptr;
+    u32 ioCap = 0;
 
     perft_stats stats{};
     std::mutex mu;
@@ -627,8 +798,8 @@ private:
     }
     u64 arena_free() const { return arenaCap > arenaTop ? arenaCap - arenaTop : 0; }
     bool alloc_level(DeviceLevel &L, u64 n);
-    int scan(const u32 *cnt, u64 n, u64 *&scanOut, u32 *&tileFirst, u64 &total);
-    int launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst,
+    int scan(const u32 *cnt, u64 n, u64 *&scanOut, u32 *&tileFirst, u64 &total, int &capLog2);
+    int launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst, int capLog2,
                     u64 itemBase, u64 itemEnd, DeviceLevel *children, unsigned long long *rootCounts);
     int process_level(const DeviceLevel &L, int remaining, unsigned long long *rootCounts);
     int process_level_tt(const DeviceLevel &L, int remaining, unsigned long long *parentAcc,
@@ -674,6 +845,28 @@ private:
     int check(cudaError_t e, const char *what);
     int sync_and_check_errors();
     int autotune(bool leaf, bool expand);
+
+    // device-driven runs captured as CUDA graphs (small single-depth batches)
+    struct DDGraph {
+        int depth = 0;
+        u32 n = 0;
+        const u64 *dPos = nullptr;
+        u64 *dOut = nullptr;
+        u64 top = 0;
+        int svL = 0, svE = 0;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        DevPlan *hTemplate = nullptr;  // pinned
+        u32 *hIds = nullptr;           // pinned
+        u64 *hFlags = nullptr;         // pinned: overflow, device error, leaf items
+    };
+    std::vector<DDGraph> ddCache;
+    bool ddEnabled = true;
+    bool ddForce = false;  // PERFT_DD_FORCE=1: skip the size estimate (tests the overflow fallback)
+    int ddGridScan = 0;
+    int run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, bool &handled);
+    int build_dd(DDGraph &G);
+    void drop_dd();
 };
 
 int Engine::check(cudaError_t e, const char *what)
@@ -800,6 +993,15 @@ int Engine::init(const perft_config &cfg)
     gridTile[MODE_EXPAND][SV_HYBRID] = occupancy_grid<MODE_EXPAND, SV_HYBRID>(nsm);
     gridTile[MODE_LEAF][SV_HYBRID] = occupancy_grid<MODE_LEAF, SV_HYBRID>(nsm);
 
+    for (auto fn : {(const void *)k_tile<MODE_LEAF, SV_KOGGE, false, true>,
+                    (const void *)k_tile<MODE_LEAF, SV_KOGGE_SPLIT, false, true>,
+                    (const void *)k_tile<MODE_EXPAND, SV_KOGGE, false, true>,
+                    (const void *)k_tile<MODE_EXPAND, SV_KOGGE_SPLIT, false, true>})
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_DYN_SMEM);
+    ddGridScan = 4 * nsm;
+    ddEnabled = !(getenv("PERFT_NO_GRAPHS") && getenv("PERFT_NO_GRAPHS")[0] == '1');
+    ddForce = getenv("PERFT_DD_FORCE") && getenv("PERFT_DD_FORCE")[0] == '1';
+
     auto pick = [](int v) { return (v >= 0 && v < SV_COUNT) ? v : SV_KOGGE; };
     svExpand = pick(cfg.sliders_expand);
     svLeaf = pick(cfg.sliders_leaf);
@@ -825,6 +1027,11 @@ void Engine::shutdown()
     if (!ready) return;
     cudaSetDevice(device);
     cudaStreamSynchronize(stream);
+    drop_dd();
+    if (ioPos) cudaFree(ioPos);
+    if (ioOut) cudaFree(ioOut);
+    ioPos = ioOut = nullptr;
+    ioCap = 0;
     cudaFree(arena);
     if (tt) cudaFree(tt);
     tt = nullptr;
@@ -851,26 +1058,30 @@ bool Engine::alloc_level(DeviceLevel &L, u64 n)
     return L.planes && L.cnt && L.root;
 }
 
-int Engine::scan(const u32 *cnt, u64 n, u64 *&scanOut, u32 *&tileFirst, u64 &total)
+int Engine::scan(const u32 *cnt, u64 n, u64 *&scanOut, u32 *&tileFirst, u64 &total, int &capLog2)
 {
     const u64 nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
-    const u64 maxTiles = (n * MAX_LEGAL_MOVES + TILE_CAP - 1) / TILE_CAP + 1;
+    const u64 maxTiles = (n * MAX_LEGAL_MOVES) / MAX_TILES_PER_NODE_DIV + 2;
     scanOut = (u64 *)alloc(8 * (n + 1));
     tileFirst = (u32 *)alloc(4 * maxTiles);
     u64 *bsum = (u64 *)alloc(8 * (nb + 1));
     if (!scanOut || !tileFirst || !bsum) return PERFT_ERR_OUT_OF_MEMORY;
     k_scan_reduce<<<(unsigned)nb, SCAN_NT, 0, stream>>>(cnt, n, bsum);
     k_scan_top<<<1, SCAN_TOP_NT, 0, stream>>>(bsum, nb, scanOut + n);
-    k_scan_apply<<<(unsigned)nb, SCAN_NT, 0, stream>>>(cnt, n, bsum, scanOut, tileFirst);
-    stats.other_launches += 3;
     ENG_TRY(cudaGetLastError());
     ENG_TRY(cudaMemcpyAsync(hPinned, scanOut + n, 8, cudaMemcpyDeviceToHost, stream));
     ENG_TRY(cudaStreamSynchronize(stream));
     total = hPinned[0];
+    // tile size: as large as possible while every resident CTA still gets tiles
+    capLog2 = TILE_CAP_LOG2;
+    while (capLog2 > TILE_MIN_LOG2 && (total >> capLog2) < 2ull * gridTile[MODE_LEAF][svLeaf]) capLog2--;
+    k_scan_apply<<<(unsigned)nb, SCAN_NT, 0, stream>>>(cnt, n, bsum, scanOut, tileFirst, capLog2);
+    stats.other_launches += 3;
+    ENG_TRY(cudaGetLastError());
     return PERFT_OK;
 }
 
-int Engine::launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst,
+int Engine::launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst, int capLog2,
                         u64 itemBase, u64 itemEnd, DeviceLevel *children,
                         unsigned long long *rootCounts)
 {
@@ -884,6 +1095,7 @@ int Engine::launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, 
     P.tileFirst = tileFirst;
     P.itemBase = itemBase;
     P.itemEnd = itemEnd;
+    P.capLog2 = capLog2;
     P.tileCounter = dCounter;
     if (children) {
         P.cpl = children->planes;
@@ -894,7 +1106,7 @@ int Engine::launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, 
     P.rootCounts = rootCounts;
     P.err = dErr;
 
-    const u64 nTiles = (itemEnd - itemBase + TILE_CAP - 1) / TILE_CAP;
+    const u64 nTiles = (itemEnd - itemBase + (1ull << capLog2) - 1) >> capLog2;
     const int sv = mode == MODE_LEAF ? svLeaf : svExpand;
     const int grid = (int)std::min<u64>((u64)gridTile[mode][sv], nTiles);
     ENG_TRY(cudaMemsetAsync(dCounter, 0, 4, stream));
@@ -931,14 +1143,15 @@ int Engine::process_level(const DeviceLevel &L, int remaining, unsigned long lon
     u64 *pscan = nullptr;
     u32 *tileFirst = nullptr;
     u64 total = 0;
-    int rc = scan(L.cnt, L.n, pscan, tileFirst, total);
+    int capLog2 = TILE_CAP_LOG2;
+    int rc = scan(L.cnt, L.n, pscan, tileFirst, total, capLog2);
     if (rc != PERFT_OK) return rc;
     if (total == 0) {
         arenaTop = mark;
         return PERFT_OK;
     }
     if (remaining == 2) {
-        rc = launch_tile(MODE_LEAF, L, pscan, tileFirst, 0, total, nullptr, rootCounts);
+        rc = launch_tile(MODE_LEAF, L, pscan, tileFirst, capLog2, 0, total, nullptr, rootCounts);
         arenaTop = mark;
         return rc;
     }
@@ -956,7 +1169,7 @@ int Engine::process_level(const DeviceLevel &L, int remaining, unsigned long lon
         const u64 cm = arenaTop;
         DeviceLevel C;
         if (!alloc_level(C, hi - lo)) return PERFT_ERR_OUT_OF_MEMORY;
-        rc = launch_tile(MODE_EXPAND, L, pscan, tileFirst, lo, hi, &C, nullptr);
+        rc = launch_tile(MODE_EXPAND, L, pscan, tileFirst, capLog2, lo, hi, &C, nullptr);
         if (rc != PERFT_OK) return rc;
         rc = process_level(C, remaining - 1, rootCounts);
         if (rc != PERFT_OK) return rc;
@@ -984,6 +1197,12 @@ int Engine::autotune(bool leaf, bool expand)
     const int keepLeaf = svLeaf, keepExpand = svExpand;
     ulonglong2 *keepTT = tt;
     tt = nullptr;  // time the kernels, not table hits
+    const bool keepDD = ddEnabled;
+    ddEnabled = false;  // the host-driven path times each launch
+    struct RestoreDD {
+        bool &slot, value;
+        ~RestoreDD() { slot = value; }
+    } restoreDD{ddEnabled, keepDD};
     struct Restore {
         ulonglong2 *&slot, *value;
         ~Restore() { slot = value; }
@@ -1072,13 +1291,14 @@ int Engine::process_level_tt(const DeviceLevel &L, int remaining, unsigned long 
     u64 *pscan = nullptr;
     u32 *tileFirst = nullptr;
     u64 total = 0;
-    int rc = scan(L.cnt, L.n, pscan, tileFirst, total);
+    int capLog2 = TILE_CAP_LOG2;
+    int rc = scan(L.cnt, L.n, pscan, tileFirst, total, capLog2);
     if (rc != PERFT_OK) return rc;
     DeviceLevel self = L;
     self.root = nullptr;  // tile sums and child links point at the parent itself
     if (total > 0) {
         if (remaining == 2) {
-            rc = launch_tile(MODE_LEAF, self, pscan, tileFirst, 0, total, nullptr, L.acc);
+            rc = launch_tile(MODE_LEAF, self, pscan, tileFirst, capLog2, 0, total, nullptr, L.acc);
             if (rc != PERFT_OK) return rc;
         } else {
             const u64 slack = std::min<u64>(64ull << 20, arenaCap / 16);
@@ -1093,7 +1313,7 @@ int Engine::process_level_tt(const DeviceLevel &L, int remaining, unsigned long 
                 const u64 cm = arenaTop;
                 DeviceLevel C;
                 if (!alloc_level_tt(C, hi - lo)) return PERFT_ERR_OUT_OF_MEMORY;
-                rc = launch_tile(MODE_EXPAND, self, pscan, tileFirst, lo, hi, &C, nullptr);
+                rc = launch_tile(MODE_EXPAND, self, pscan, tileFirst, capLog2, lo, hi, &C, nullptr);
                 if (rc != PERFT_OK) return rc;
                 rc = process_level_tt(C, remaining - 1, L.acc, nullptr);
                 if (rc != PERFT_OK) return rc;
@@ -1113,6 +1333,186 @@ int Engine::process_level_tt(const DeviceLevel &L, int remaining, unsigned long 
     return PERFT_OK;
 }
 
+void Engine::drop_dd()
+{
+    for (DDGraph &G : ddCache) {
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        if (G.graph) cudaGraphDestroy(G.graph);
+        cudaFreeHost(G.hTemplate);
+        cudaFreeHost(G.hIds);
+        cudaFreeHost(G.hFlags);
+    }
+    ddCache.clear();
+}
+
+// Captures one device-driven perft of G.n roots at G.depth.  Every buffer the
+// graph reads is re-initialised inside it (plan, root ids, outputs), so the
+// region above the arena top may be reused by other calls between replays.
+int Engine::build_dd(DDGraph &G)
+{
+    const u64 n = G.n;
+    const u64 off0 = (arenaTop + 255) & ~255ULL;
+    char *base = arena + off0;
+    const u64 cap = arenaCap - off0;
+    u64 bump = 0;
+    auto place = [&](u64 bytes) -> char * {
+        const u64 a = (bump + 255) & ~255ULL;
+        bump = a + bytes;
+        return base + a;
+    };
+    DevPlan *dPlan = (DevPlan *)place(sizeof(DevPlan));
+    u32 *dIds = (u32 *)place(4 * n);
+    LevelDesc L0{};
+    L0.n = n;
+    L0.stride = (n + 31) & ~31ULL;
+    L0.planes = (u64 *)place(48 * L0.stride);
+    L0.cnt = (u32 *)place(4 * L0.stride);
+    L0.root = (u32 *)place(4 * L0.stride);
+    L0.pscan = (u64 *)place(8 * (n + 1));
+    L0.tileFirst = (u32 *)place(4 * ((n * MAX_LEGAL_MOVES) / MAX_TILES_PER_NODE_DIV + 2));
+    L0.bsum = (u64 *)place(8 * ((n + SCAN_CHUNK - 1) / SCAN_CHUNK + 1));
+    if (bump > cap) return PERFT_ERR_OUT_OF_MEMORY;
+
+    ENG_TRY(cudaMallocHost(&G.hTemplate, sizeof(DevPlan)));
+    ENG_TRY(cudaMallocHost(&G.hIds, 4 * n));
+    ENG_TRY(cudaMallocHost(&G.hFlags, 64));
+    memset(G.hTemplate, 0, sizeof(DevPlan));
+    G.hTemplate->base = base;
+    G.hTemplate->cap = cap;
+    G.hTemplate->bump = bump;
+    G.hTemplate->tileTarget = 2 * gridTile[MODE_LEAF][G.svL];
+    G.hTemplate->lv[0] = L0;
+    for (u32 i = 0; i < n; i++) G.hIds[i] = i;
+
+    const int d = G.depth;
+    ENG_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(dPlan, G.hTemplate, sizeof(DevPlan), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(dIds, G.hIds, 4 * n, cudaMemcpyHostToDevice, stream);
+    cudaMemsetAsync(G.dOut, 0, 8 * n, stream);
+    cudaMemsetAsync(dErr, 0, 4, stream);
+    k_init_roots<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(G.dPos, dIds, (u32)n, L0.planes, L0.stride, L0.cnt,
+                                                                  L0.root, d, (unsigned long long *)G.dOut, dErr);
+    for (int lv = 0; lv <= d - 2; lv++) {
+        const int last = lv == d - 2;
+        k_dd_scan_reduce<<<ddGridScan, SCAN_NT, 0, stream>>>(dPlan, lv);
+        k_dd_scan_top<<<1, SCAN_TOP_NT, 0, stream>>>(dPlan, lv, last);
+        k_dd_scan_apply<<<ddGridScan, SCAN_NT, 0, stream>>>(dPlan, lv);
+        cudaMemsetAsync(dCounter, 0, 4, stream);
+        TileParams P;
+        memset(&P, 0, sizeof P);
+        P.dpar = &dPlan->lv[lv];
+        P.dch = last ? nullptr : &dPlan->lv[lv + 1];
+        P.tileCounter = dCounter;
+        P.rootCounts = (unsigned long long *)G.dOut;
+        P.err = dErr;
+        const int sv = last ? G.svL : G.svE;
+        const int grid = gridTile[last ? MODE_LEAF : MODE_EXPAND][sv];
+        if (last) {
+            if (sv == SV_KOGGE_SPLIT) k_tile<MODE_LEAF, SV_KOGGE_SPLIT, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
+            else k_tile<MODE_LEAF, SV_KOGGE, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
+        } else {
+            if (sv == SV_KOGGE_SPLIT) k_tile<MODE_EXPAND, SV_KOGGE_SPLIT, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
+            else k_tile<MODE_EXPAND, SV_KOGGE, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
+        }
+    }
+    cudaMemcpyAsync(&G.hFlags[0], &dPlan->overflow, 4, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(&G.hFlags[1], dErr, 4, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(&G.hFlags[2], &dPlan->lv[d - 2].total, 8, cudaMemcpyDeviceToHost, stream);
+    const cudaError_t ce = cudaStreamEndCapture(stream, &G.graph);
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        return check(ce, "capture of the device-driven perft");
+    }
+    ENG_TRY(cudaGraphInstantiate(&G.exec, G.graph, 0));
+    return PERFT_OK;
+}
+
+// Single-depth batches whose predicted tree is small run as one replayed
+// graph: the launch sequence is fixed and the sizes live on the device, so
+// the host only waits once.  `handled` stays false when the batch is not
+// eligible or the device plan overflowed; the caller then runs the
+// host-driven path.
+int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, bool &handled)
+{
+    handled = false;
+    if (!ddEnabled || tt || n == 0) return PERFT_OK;
+    const int d = depths[0];
+    for (u32 i = 1; i < n; i++)
+        if (depths[i] != d) return PERFT_OK;
+    if (d < 2 || d > DD_MAX_LEVELS) return PERFT_OK;
+    auto ddSv = [](int v) { return v == SV_KOGGE || v == SV_KOGGE_SPLIT; };
+    if (!ddSv(svLeaf) || !ddSv(svExpand)) return PERFT_OK;
+    double est = (double)n * 130.0;
+    for (int k = 2; k < d; k++) est *= 40.0;
+    if (est > 0.25 * (double)arena_free() && !ddForce) return PERFT_OK;
+
+    DDGraph *G = nullptr;
+    for (DDGraph &g : ddCache)
+        if (g.depth == d && g.n == n && g.dPos == dPos && g.dOut == dOut && g.top == arenaTop && g.svL == svLeaf &&
+            g.svE == svExpand)
+            G = &g;
+    if (!G) {
+        if (ddCache.size() >= 16) {
+            DDGraph &old = ddCache.front();
+            if (old.exec) cudaGraphExecDestroy(old.exec);
+            if (old.graph) cudaGraphDestroy(old.graph);
+            cudaFreeHost(old.hTemplate);
+            cudaFreeHost(old.hIds);
+            cudaFreeHost(old.hFlags);
+            ddCache.erase(ddCache.begin());
+        }
+        ddCache.emplace_back();
+        G = &ddCache.back();
+        G->depth = d;
+        G->n = n;
+        G->dPos = dPos;
+        G->dOut = dOut;
+        G->top = arenaTop;
+        G->svL = svLeaf;
+        G->svE = svExpand;
+        const int rc = build_dd(*G);
+        if (rc != PERFT_OK) {
+            drop_dd();
+            return rc == PERFT_ERR_OUT_OF_MEMORY ? PERFT_OK : rc;
+        }
+    }
+    ENG_TRY(cudaGraphLaunch(G->exec, stream));
+    ENG_TRY(cudaStreamSynchronize(stream));
+    stats.other_launches += 1 + 3ull * (d - 1);
+    stats.expand_launches += d - 2;
+    stats.leaf_launches += 1;
+    stats.graph_launches += 1;
+    if ((u32)G->hFlags[0]) return PERFT_OK;  // overflow: rerun host-driven
+    const u32 e = (u32)G->hFlags[1];
+    if (e & DERR_BAD_POSITION) return PERFT_ERR_INVALID_ARG;
+    if (e) return PERFT_ERR_INTERNAL;
+    stats.leaf_items += G->hFlags[2];
+    handled = true;
+    return PERFT_OK;
+}
+
+int Engine::run_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *out)
+{
+    if (n > ioCap) {
+        if (ioPos) cudaFree(ioPos);
+        if (ioOut) cudaFree(ioOut);
+        ioPos = ioOut = nullptr;
+        ioCap = 0;
+        u32 cap = 1024;
+        while (cap < n) cap *= 2;
+        ENG_TRY(cudaMalloc(&ioPos, 48ull * cap));
+        ENG_TRY(cudaMalloc(&ioOut, 8ull * cap));
+        ioCap = cap;
+        drop_dd();
+    }
+    ENG_TRY(cudaMemcpyAsync(ioPos, pos, 48ull * n, cudaMemcpyHostToDevice, stream));
+    const int rc = run_batch(ioPos, depths, n, ioOut);
+    if (rc != PERFT_OK) return rc;
+    ENG_TRY(cudaMemcpyAsync(out, ioOut, 8ull * n, cudaMemcpyDeviceToHost, stream));
+    ENG_TRY(cudaStreamSynchronize(stream));
+    return PERFT_OK;
+}
+
 int Engine::sync_and_check_errors()
 {
     ENG_TRY(cudaMemcpyAsync(hPinned + 1, dErr, 4, cudaMemcpyDeviceToHost, stream));
@@ -1126,6 +1526,11 @@ int Engine::sync_and_check_errors()
 int Engine::run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut)
 {
     ENG_TRY(cudaSetDevice(device));
+    {
+        bool handled = false;
+        const int rc = run_dd(dPos, depths, n, dOut, handled);
+        if (rc != PERFT_OK || handled) return rc;
+    }
     const u64 mark0 = arenaTop;
     unsigned long long *rootCounts = (unsigned long long *)dOut;
     ENG_TRY(cudaMemsetAsync(rootCounts, 0, 8ull * n, stream));
@@ -1190,20 +1595,7 @@ int pg::engine_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *out
         if (validate_pos48(pos + 6ull * i) != 0) return PERFT_ERR_INVALID_ARG;
         if (depths[i] > 20) return PERFT_ERR_INVALID_ARG;
     }
-    u64 *dPos = nullptr, *dOut = nullptr;
-    if (cudaMalloc(&dPos, 48ull * n) != cudaSuccess) return PERFT_ERR_OUT_OF_MEMORY;
-    if (cudaMalloc(&dOut, 8ull * n) != cudaSuccess) {
-        cudaFree(dPos);
-        return PERFT_ERR_OUT_OF_MEMORY;
-    }
-    int rc = PERFT_OK;
-    if (cudaMemcpy(dPos, pos, 48ull * n, cudaMemcpyHostToDevice) != cudaSuccess) rc = PERFT_ERR_CUDA;
-    if (rc == PERFT_OK) rc = E.run_batch(dPos, depths, n, dOut);
-    if (rc == PERFT_OK && cudaMemcpy(out, dOut, 8ull * n, cudaMemcpyDeviceToHost) != cudaSuccess)
-        rc = PERFT_ERR_CUDA;
-    cudaFree(dPos);
-    cudaFree(dOut);
-    return rc;
+    return E.run_batch_host(pos, depths, n, out);
 }
 
 extern "C" {
@@ -1486,7 +1878,7 @@ struct NoallocRun {
         if (!scanOut || !tileFirst || !bsum) return PERFT_ERR_OUT_OF_MEMORY;
         k_scan_reduce<<<(unsigned)nb, SCAN_NT, 0, st>>>(cnt, n, bsum);
         k_scan_top<<<1, SCAN_TOP_NT, 0, st>>>(bsum, nb, scanOut + n);
-        k_scan_apply<<<(unsigned)nb, SCAN_NT, 0, st>>>(cnt, n, bsum, scanOut, tileFirst);
+        k_scan_apply<<<(unsigned)nb, SCAN_NT, 0, st>>>(cnt, n, bsum, scanOut, tileFirst, TILE_CAP_LOG2);
         if (cudaGetLastError() != cudaSuccess) return PERFT_ERR_CUDA;
         return read_u64(scanOut + n, total);
     }
@@ -1504,6 +1896,7 @@ struct NoallocRun {
         P.tileFirst = tileFirst;
         P.itemBase = 0;
         P.itemEnd = total;
+        P.capLog2 = TILE_CAP_LOG2;
         P.tileCounter = counter;
         if (ch) {
             P.cpl = ch->planes;

@@ -401,7 +401,7 @@ int Server::scan_level(ServeLevel &S)
 {
     const u64 n = S.L.n;
     const u64 nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
-    const u64 maxTiles = (n * MAX_LEGAL_MOVES + TILE_CAP - 1) / TILE_CAP + 1;
+    const u64 maxTiles = (n * MAX_LEGAL_MOVES) / MAX_TILES_PER_NODE_DIV + 2;
     S.pscan = (u64 *)take(8 * (n + 1), S.mem);
     S.tileFirst = (u32 *)take(4 * maxTiles, S.mem);
     std::vector<std::pair<u64, u64>> tmp;
@@ -412,7 +412,7 @@ int Server::scan_level(ServeLevel &S)
     }
     k_scan_reduce<<<(unsigned)nb, SCAN_NT, 0, st>>>(S.L.cnt, n, bsum);
     k_scan_top<<<1, SCAN_TOP_NT, 0, st>>>(bsum, nb, S.pscan + n);
-    k_scan_apply<<<(unsigned)nb, SCAN_NT, 0, st>>>(S.L.cnt, n, bsum, S.pscan, S.tileFirst);
+    k_scan_apply<<<(unsigned)nb, SCAN_NT, 0, st>>>(S.L.cnt, n, bsum, S.pscan, S.tileFirst, TILE_CAP_LOG2);
     k_serve_zero_parents<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(S.L.cnt, S.L.root, n, pending);
     launches += 4;
     give_back(tmp);
@@ -436,6 +436,7 @@ int Server::launch(int mode, ServeLevel &S, u64 lo, u64 hi, DeviceLevel *child)
     P.tileFirst = S.tileFirst;
     P.itemBase = lo;
     P.itemEnd = hi;
+    P.capLog2 = TILE_CAP_LOG2;
     P.tileCounter = dCounter;
     if (child) {
         P.cpl = child->planes;

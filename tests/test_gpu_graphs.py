@@ -1,0 +1,61 @@
+"""Device-driven perft replayed as a CUDA graph: identical counts to the
+host-driven path, graph reuse across calls, and the overflow fallback."""
+import os
+
+import numpy as np
+import pytest
+
+from tests._oracle import pos48_from_hex
+
+pytestmark = pytest.mark.gpu
+
+
+def _reinit(engine, **env):
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        engine.init(device=0, arena_bytes=env.pop("_arena", 4 << 30) if "_arena" in env else 4 << 30)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+def test_graph_path_matches_host_path(engine, golden):
+    start = next(e for e in golden if e["name"] == "initial_position")
+    p = pos48_from_hex(start["pos48"])
+    pos = engine.random_playouts(seed=71, n=32, min_plies=2, max_plies=40)
+    try:
+        _reinit(engine, PERFT_NO_GRAPHS="1")
+        host = [engine.perft_batch(pos, d) for d in (2, 3, 4)]
+        assert engine.stats()["graph_launches"] == 0
+        _reinit(engine, PERFT_NO_GRAPHS="0")
+        engine.reset_stats()
+        for _ in range(3):  # first call captures, later calls replay
+            dd = [engine.perft_batch(pos, d) for d in (2, 3, 4)]
+            assert all(np.array_equal(a, b) for a, b in zip(host, dd))
+            assert engine.perft(p, 5) == int(start["counts"]["5"])
+        assert engine.stats()["graph_launches"] >= 12
+    finally:
+        engine.init(device=0, arena_bytes=8 << 30)
+
+
+def test_graph_overflow_falls_back(engine, golden):
+    """With the size estimate disabled and a 64 MiB arena, the device plan for
+    perft(6) of the initial position overflows; the host path recomputes."""
+    start = next(e for e in golden if e["name"] == "initial_position")
+    p = pos48_from_hex(start["pos48"])
+    old = os.environ.get("PERFT_DD_FORCE")
+    os.environ["PERFT_DD_FORCE"] = "1"
+    try:
+        engine.init(device=0, arena_bytes=64 << 20)
+        assert engine.perft(p, 6) == int(start["counts"]["6"])
+        assert engine.perft(p, 4) == int(start["counts"]["4"])
+    finally:
+        if old is None:
+            os.environ.pop("PERFT_DD_FORCE", None)
+        else:
+            os.environ["PERFT_DD_FORCE"] = old
+        engine.init(device=0, arena_bytes=8 << 30)
