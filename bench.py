@@ -225,6 +225,7 @@ def run_reference(args):
 def run_ours(args):
     import torch
     import perft_gpu_b200 as pg
+    from perft_gpu_b200.shard import max_sum_over_ranks
 
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
@@ -294,14 +295,9 @@ def run_ours(args):
     e_ms = e_start.elapsed_time(e_end)
     stable = stable and bool(np.array_equal(host_out, counts))
 
-    # ---- reductions over ranks
-    t = torch.tensor([ms, e_ms], dtype=torch.float64, device="cuda")
-    tot = torch.tensor([leaves_per_step], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-    ms_max, e_ms_max = float(t[0]), float(t[1])
-    total_leaves = float(tot[0]) * args.steps
+    # ---- reductions over ranks: slowest rank's times, all ranks' leaves
+    (ms_max, e_ms_max), (tot,) = max_sum_over_ranks([ms, e_ms], [leaves_per_step], device="cuda")
+    total_leaves = tot * args.steps
 
     if rank != 0:
         if dist:

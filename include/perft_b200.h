@@ -153,6 +153,28 @@ int perft_serve_poll(uint64_t ticket, uint64_t *count, double *latency_s);
 int perft_serve_wait(uint64_t ticket, double timeout_s, uint64_t *count, double *latency_s);
 int perft_serve_get_stats(perft_serve_stats *out);
 
+/* Deep perft by host root split (perft 11+): for every legal root move the
+ * distinct positions split_plies below it are merged with their path counts
+ * (a host transposition merge, like the reference's complete TT,
+ * launcher.h:585-697) and searched on the GPU at the remaining depth.
+ * moves/counts (optional, 256 entries) receive the per-move subtotals, the
+ * divided perft of launcher.h:1344-1351. */
+int perft_deep(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, char (*moves)[6],
+               uint64_t *counts, uint32_t *n_moves, uint64_t *total);
+/* One shard of perft_deep: only frontier boards i with i % n_shards == shard
+ * are searched.  The frontier order is deterministic, so the per-move
+ * subtotals of shards 0..n_shards-1 (one process per GPU) sum to perft_deep's:
+ * the multi-GPU root split of launcher.h:476-583 with one 8-byte-per-move sum
+ * as the only exchange. */
+int perft_deep_shard(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, uint32_t shard,
+                     uint32_t n_shards, char (*moves)[6], uint64_t *counts, uint32_t *n_moves,
+                     uint64_t *total);
+
+/* Records mode (launcher.h:1579-1695): each line of in_path is a FEN ending
+ * with an occurrence count; "<line> <perft> <perft*count>" is appended to
+ * in_path.op.  Lines already in the output are skipped (resume). */
+int perft_records(const char *in_path, uint32_t depth, uint32_t batch, uint64_t *records_done);
+
 /* ------------------------------------------------------- host utilities */
 
 /* FEN -> position: Utils::readFENString + board088ToHexBB

@@ -145,6 +145,11 @@ def _load():
         "perft_serve_wait": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_double, P(ctypes.c_uint64),
                                             P(ctypes.c_double)]),
         "perft_serve_get_stats": (ctypes.c_int, [P(ServeStats)]),
+        "perft_deep": (ctypes.c_int, [P(_Pos48), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, u64p,
+                                      P(ctypes.c_uint32), u64p]),
+        "perft_deep_shard": (ctypes.c_int, [P(_Pos48), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                            ctypes.c_uint32, ctypes.c_void_p, u64p, P(ctypes.c_uint32), u64p]),
+        "perft_records": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, u64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -263,6 +268,28 @@ def reset_stats() -> None:
 
 def tt_clear() -> None:
     _check(lib().perft_tt_clear(), "perft_tt_clear")
+
+
+def deep(pos, depth: int, split_plies: int = 2, shard: int = 0, n_shards: int = 1):
+    """(total, {uci move: subtotal}) by host root split with transposition
+    merging and GPU batches.  With n_shards > 1 only this shard's frontier
+    boards are searched; the shards' results sum to the full count."""
+    p = _pos(pos)
+    moves = (ctypes.c_char * (6 * 256))()
+    counts = (ctypes.c_uint64 * 256)()
+    n, total = ctypes.c_uint32(0), ctypes.c_uint64(0)
+    _check(lib().perft_deep_shard(ctypes.byref(p), int(depth), int(split_plies), int(shard), int(n_shards), moves,
+                                  counts, ctypes.byref(n), ctypes.byref(total)), "perft_deep_shard")
+    raw = bytes(moves)
+    div = {raw[6 * i:6 * i + 6].split(b"\0")[0].decode(): int(counts[i]) for i in range(n.value)}
+    return int(total.value), div
+
+
+def records(path: str, depth: int, batch: int = 4096) -> int:
+    """Records mode; returns the number of records processed by this call."""
+    done = ctypes.c_uint64(0)
+    _check(lib().perft_records(path.encode(), int(depth), int(batch), ctypes.byref(done)), "perft_records")
+    return int(done.value)
 
 
 # ---------------------------------------------------------------- serving

@@ -11,6 +11,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libperft_b200.so")
 PROBE_LIB = os.path.join(HERE, "libperft_probe.so")
+CLI = os.path.join(HERE, "perft_gpu")
 
 SOURCES = ["engine.cu", "tables.cpp", "host.cpp"]
 HEADERS = ["movegen.cuh", "serve.cuh", os.path.join("..", "..", "include", "perft_b200.h")]
@@ -50,12 +51,22 @@ def build_variant(out, defines, verbose=False):
     return out
 
 
+def _cli():
+    """The perft_gpu command-line program, linked against the engine library."""
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", CLI, os.path.join(CSRC, "cli.cpp"),
+                    "-L", HERE, "-lperft_b200", "-Wl,-rpath,$ORIGIN"], check=True)
+
+
 def build(verbose=False, force=False):
-    """Compiles the engine and the integer-peak probe libraries (sm_100a)."""
+    """Compiles the engine and the integer-peak probe libraries (sm_100a) and
+    the perft_gpu program."""
     if force or not up_to_date(LIB, SOURCES + HEADERS):
         _nvcc(LIB, SOURCES, verbose)
     if force or not up_to_date(PROBE_LIB, ["int_peak.cu"]):
         _nvcc(PROBE_LIB, ["int_peak.cu"], verbose)
+    if force or not up_to_date(CLI, ["cli.cpp", os.path.join("..", "..", "include", "perft_b200.h")]) \
+            or os.path.getmtime(CLI) < os.path.getmtime(LIB):
+        _cli()
     return LIB
 
 

@@ -1,0 +1,266 @@
+// Command-line front end over the C ABI (include/perft_b200.h).
+//
+//   perft_gpu <fen|startpos> <depth> [<gpus>] [<launchdepth>]
+//       The reference's process CLI (perft.cu:14-164): prints Perft(NN) for
+//       every depth from 3 (or depth, if smaller) up to <depth>, each with
+//       its wall time.  Above depth 10 the root moves' subtotals are printed
+//       first, as the reference's divided perft does (launcher.h:1344-1351),
+//       computed by the host root split with transposition merging.  <gpus>
+//       is accepted for command-line compatibility; one process drives one
+//       GPU (CUDA_VISIBLE_DEVICES / PERFT_DEVICE pick it).  <launchdepth> is
+//       accepted and ignored: level sizes are planned from measured counts.
+//   perft_gpu --records <file> [<depth>]
+//       Records mode (launcher.h:1579-1695): "<line> <perft> <perft*count>"
+//       per input line appended to <file>.op, resuming after the lines
+//       already written.  Depth defaults to 7.
+//   perft_gpu --uci
+//       A minimal UCI loop (uci, isready, ucinewgame, position startpos|fen
+//       ... [moves ...], go perft N, d, quit).  The reference's UCI is a stub
+//       (UciInterface.cpp:7); "go perft" prints one "move: count" line per
+//       root move, then "Nodes searched: N".
+#include <chrono>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <string>
+#include <vector>
+
+#include "../../include/perft_b200.h"
+
+namespace {
+
+const char *START_FEN = "rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1";
+bool g_ready = false;
+
+int ensure_init()
+{
+    if (g_ready) return PERFT_OK;
+    perft_config cfg;
+    perft_config_default(&cfg);
+    if (const char *d = getenv("PERFT_DEVICE")) cfg.device = atoi(d);
+    if (const char *a = getenv("PERFT_ARENA_GB")) cfg.arena_bytes = (uint64_t)(atof(a) * (1ull << 30));
+    if (const char *t = getenv("PERFT_TT_LOG2")) cfg.tt_log2_entries = (uint32_t)atoi(t);
+    const int rc = perft_init(&cfg);
+    if (rc != PERFT_OK) {
+        fprintf(stderr, "perft_init failed: %s\n", perft_status_string(rc));
+        return rc;
+    }
+    g_ready = true;
+    return PERFT_OK;
+}
+
+double now_s()
+{
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+void usage()
+{
+    printf("Usage perft_gpu <fen> <depth> [<gpus>] [<launchdepth>]\n"
+           "      perft_gpu --records <file> [<depth>]\n"
+           "      perft_gpu --uci\n");
+}
+
+// Divided count of pos at depth: one subtotal per root move.
+int divided(const perft_pos48 &pos, uint32_t depth, std::vector<std::string> &moves,
+            std::vector<uint64_t> &counts, uint64_t *total)
+{
+    char mv[256][6];
+    uint64_t c[256];
+    uint32_t n = 0;
+    int rc;
+    if (depth > 10) {
+        rc = perft_deep(&pos, depth, depth - 7 < 4 ? depth - 7 : 4, mv, c, &n, total);
+    } else {
+        rc = perft_divide(&pos, depth, mv, c, &n);
+        *total = 0;
+        for (uint32_t i = 0; rc == PERFT_OK && i < n; i++) *total += c[i];
+    }
+    if (rc != PERFT_OK) return rc;
+    moves.clear();
+    counts.clear();
+    for (uint32_t i = 0; i < n; i++) {
+        moves.emplace_back(mv[i]);
+        counts.push_back(c[i]);
+    }
+    return PERFT_OK;
+}
+
+int run_cli(int argc, char **argv)
+{
+    std::string fen = argv[1];
+    if (fen == "startpos" || fen.size() <= 5) fen = START_FEN;
+    const int maxDepth = atoi(argv[2]);
+    if (maxDepth < 0 || maxDepth > 30) {
+        usage();
+        return 2;
+    }
+    perft_pos48 pos;
+    int rc = perft_fen_to_pos(fen.c_str(), &pos);
+    if (rc != PERFT_OK) {
+        fprintf(stderr, "bad FEN: %s\n", perft_status_string(rc));
+        return 2;
+    }
+    if ((rc = ensure_init()) != PERFT_OK) return 1;
+    char canon[128];
+    perft_pos_to_fen(&pos, canon, sizeof canon);
+    printf("%s\n", canon);
+    const int minDepth = maxDepth < 3 ? maxDepth : 3;
+    for (int d = minDepth; d <= maxDepth; d++) {
+        const double t0 = now_s();
+        uint64_t total = 0;
+        if (d > 10) {
+            std::vector<std::string> mv;
+            std::vector<uint64_t> c;
+            rc = divided(pos, (uint32_t)d, mv, c, &total);
+            if (rc == PERFT_OK)
+                for (size_t i = 0; i < mv.size(); i++) printf("%s   %20llu\n", mv[i].c_str(), (unsigned long long)c[i]);
+        } else {
+            rc = perft(&pos, (uint32_t)d, &total);
+        }
+        if (rc != PERFT_OK) {
+            fprintf(stderr, "perft(%d) failed: %s\n", d, perft_status_string(rc));
+            return 1;
+        }
+        printf("Perft(%02d):%20llu, time: %8g s\n", d, (unsigned long long)total, now_s() - t0);
+        fflush(stdout);
+    }
+    return 0;
+}
+
+int run_records(int argc, char **argv)
+{
+    if (argc < 3) {
+        usage();
+        return 2;
+    }
+    const uint32_t depth = argc >= 4 ? (uint32_t)atoi(argv[3]) : 7;
+    if (ensure_init() != PERFT_OK) return 1;
+    printf("filename of op: %s.op\n", argv[2]);
+    const double t0 = now_s();
+    uint64_t done = 0;
+    const int rc = perft_records(argv[2], depth, 0, &done);
+    if (rc != PERFT_OK) {
+        fprintf(stderr, "records failed: %s\n", perft_status_string(rc));
+        return 1;
+    }
+    const double t = now_s() - t0;
+    printf("Records done: %llu, Total: %g seconds, Avg: %g seconds\n", (unsigned long long)done, t,
+           done ? t / (double)done : 0.0);
+    return 0;
+}
+
+// Splits a line into whitespace-separated tokens.
+std::vector<std::string> tokens(const char *line)
+{
+    std::vector<std::string> out;
+    std::string cur;
+    for (const char *p = line; *p; p++) {
+        if (*p == ' ' || *p == '\t' || *p == '\n' || *p == '\r') {
+            if (!cur.empty()) out.push_back(cur);
+            cur.clear();
+        } else {
+            cur += *p;
+        }
+    }
+    if (!cur.empty()) out.push_back(cur);
+    return out;
+}
+
+int run_uci()
+{
+    perft_pos48 pos;
+    perft_fen_to_pos(START_FEN, &pos);
+    char line[8192];
+    while (fgets(line, sizeof line, stdin)) {
+        const std::vector<std::string> t = tokens(line);
+        if (t.empty()) continue;
+        const std::string &cmd = t[0];
+        if (cmd == "quit") {
+            break;
+        } else if (cmd == "uci") {
+            printf("id name perft_gpu_b200\nid author perft_gpu_b200 contributors\nuciok\n");
+        } else if (cmd == "isready") {
+            printf("readyok\n");
+        } else if (cmd == "ucinewgame") {
+            perft_fen_to_pos(START_FEN, &pos);
+        } else if (cmd == "position" && t.size() >= 2) {
+            size_t i = 1;
+            std::string fen;
+            if (t[1] == "startpos") {
+                fen = START_FEN;
+                i = 2;
+            } else if (t[1] == "fen") {
+                for (i = 2; i < t.size() && t[i] != "moves"; i++) fen += (fen.empty() ? "" : " ") + t[i];
+            }
+            perft_pos48 p;
+            if (perft_fen_to_pos(fen.c_str(), &p) != PERFT_OK) {
+                printf("info string bad fen\n");
+                fflush(stdout);
+                continue;
+            }
+            bool ok = true;
+            if (i < t.size() && t[i] == "moves")
+                for (i++; i < t.size() && ok; i++) ok = perft_apply_uci_move(&p, t[i].c_str()) == PERFT_OK;
+            if (!ok)
+                printf("info string illegal move %s\n", t[i - 1].c_str());
+            else
+                pos = p;
+        } else if (cmd == "d") {
+            char fen[128];
+            perft_pos_to_fen(&pos, fen, sizeof fen);
+            printf("Fen: %s\n", fen);
+        } else if (cmd == "go" && t.size() >= 3 && t[1] == "perft") {
+            const int depth = atoi(t[2].c_str());
+            if (depth < 1 || depth > 30) {
+                printf("info string bad depth\n");
+            } else if (ensure_init() == PERFT_OK) {
+                std::vector<std::string> mv;
+                std::vector<uint64_t> c;
+                uint64_t total = 0;
+                const double t0 = now_s();
+                const int rc = divided(pos, (uint32_t)depth, mv, c, &total);
+                if (rc != PERFT_OK) {
+                    printf("info string perft failed: %s\n", perft_status_string(rc));
+                } else {
+                    for (size_t k = 0; k < mv.size(); k++) printf("%s: %llu\n", mv[k].c_str(), (unsigned long long)c[k]);
+                    const double dt = now_s() - t0;
+                    printf("\nNodes searched: %llu\ninfo string time %g s, %g leaves/s\n\n", (unsigned long long)total,
+                           dt, dt > 0 ? (double)total / dt : 0.0);
+                }
+            } else {
+                printf("info string no GPU engine\n");
+            }
+        } else {
+            printf("info string unknown command %s\n", cmd.c_str());
+        }
+        fflush(stdout);
+    }
+    if (g_ready) perft_shutdown();
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+    if (argc >= 2 && (!strcmp(argv[1], "--help") || !strcmp(argv[1], "-h"))) {
+        usage();
+        return 0;
+    }
+    if (argc >= 2 && !strcmp(argv[1], "--uci")) return run_uci();
+    if (argc >= 2 && !strcmp(argv[1], "--records")) return run_records(argc, argv);
+    if (argc < 3) {
+        usage();
+        printf("\nAs no parameters were provided... running the start position to depth 5\n");
+        static char a0[] = "perft_gpu", a1[] = "startpos", a2[] = "5";
+        char *def[] = {a0, a1, a2};
+        const int rc = run_cli(3, def);
+        if (g_ready) perft_shutdown();
+        return rc;
+    }
+    const int rc = run_cli(argc, argv);
+    if (g_ready) perft_shutdown();
+    return rc;
+}

@@ -2,11 +2,14 @@
 // strings, divided perft, seeded playout positions.  They use the host build
 // of the move generator for move lists only; every leaf count is computed by
 // the GPU engine (engine.cu).
+#include <algorithm>
 #include <random>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "../../include/perft_b200.h"
@@ -58,6 +61,83 @@ void move_to_uci(const Board &b, u32 mv, char out[6])
 }
 
 bool board_ok(const perft_pos48 *p) { return validate_pos48(p->bb) == 0; }
+
+// Frontier of a deep search: the distinct side-relative boards a fixed number
+// of plies below the root moves, each searched once however many move paths
+// (from however many root moves) reach it.  This host-side transposition merge
+// plays the role of the reference's complete hash tables for perft 11+
+// (launcher.h:585-697); the side bit is dropped from the key because counts of
+// a side-relative board do not depend on the real colour.
+struct BoardKey {
+    u64 w[6];
+    bool operator==(const BoardKey &o) const { return memcmp(w, o.w, sizeof w) == 0; }
+};
+struct BoardKeyHash {
+    size_t operator()(const BoardKey &k) const
+    {
+        u64 h = 0x9E3779B97F4A7C15ULL;
+        for (u64 x : k.w) h = (h ^ x) * 0xBF58476D1CE4E5B9ULL;
+        return (size_t)(h ^ (h >> 31));
+    }
+};
+
+struct Frontier {
+    std::unordered_map<BoardKey, u32, BoardKeyHash> index;
+    std::vector<BoardKey> boards;
+    // (distinct board, path count) per root move
+    std::vector<std::unordered_map<u32, u64>> paths;
+
+    void add(u32 root, const Board &b, u64 mult)
+    {
+        const BoardKey k{{b.mine, b.pawns & ~SIDE_BIT, b.knights, b.bq, b.rq, b.kings}};
+        auto it = index.find(k);
+        u32 id;
+        if (it == index.end()) {
+            id = (u32)boards.size();
+            index.emplace(k, id);
+            boards.push_back(k);
+        } else {
+            id = it->second;
+        }
+        paths[root][id] += mult;
+    }
+    void enumerate(u32 root, const Board &b, u32 plies)
+    {
+        if (plies == 0) {
+            add(root, b, 1);
+            return;
+        }
+        for (u32 m : legal_moves(b)) enumerate(root, make_child(b, m), plies - 1);
+    }
+};
+
+// perft(depth) of the distinct frontier boards whose index is congruent to
+// `shard` modulo `n_shards`, in GPU batches; the others are left at 0.
+int frontier_counts(const Frontier &f, u32 depth, u32 shard, u32 n_shards, std::vector<u64> &counts)
+{
+    constexpr u32 CHUNK = 1u << 18;
+    const u32 total = (u32)f.boards.size();
+    counts.assign(total, 0);
+    std::vector<u32> ids;
+    for (u32 i = shard; i < total; i += n_shards) ids.push_back(i);
+    std::vector<u64> pos, out;
+    std::vector<uint8_t> depths;
+    for (size_t lo = 0; lo < ids.size(); lo += CHUNK) {
+        const u32 n = (u32)std::min<size_t>(CHUNK, ids.size() - lo);
+        pos.resize(6ull * n);
+        for (u32 i = 0; i < n; i++) {
+            Board b;
+            memcpy(&b, f.boards[ids[lo + i]].w, sizeof b);
+            to_pos48(b, &pos[6ull * i]);
+        }
+        depths.assign(n, (uint8_t)depth);
+        out.assign(n, 0);
+        const int rc = engine_batch_host(pos.data(), depths.data(), n, out.data());
+        if (rc != PERFT_OK) return rc;
+        for (u32 i = 0; i < n; i++) counts[ids[lo + i]] = out[i];
+    }
+    return PERFT_OK;
+}
 
 }  // namespace
 
@@ -258,6 +338,120 @@ int perft_random_playouts(uint64_t seed, uint32_t n, uint32_t min_plies, uint32_
         made++;
     }
     return PERFT_OK;
+}
+
+// Deep perft by host root split: the distinct positions `split_plies` below
+// the root moves are merged across all root moves and searched once each on
+// the GPU at the remaining depth; per-move subtotals weight each board's count
+// by its path count.  They are the divided perft the reference prints for deep
+// runs (launcher.h:1181-1450).  split_plies is clamped to depth - 1.  With
+// n_shards > 1 only every n_shards-th frontier board (from `shard`) is
+// searched, so the per-move subtotals of shards 0..n_shards-1 sum to the full
+// result: the multi-GPU root split, one process per GPU (launcher.h:476-583).
+int perft_deep_shard(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, uint32_t shard,
+                     uint32_t n_shards, char (*moves)[6], uint64_t *counts, uint32_t *n_moves, uint64_t *total)
+{
+    if (!pos || !total || depth < 1 || depth > 30) return PERFT_ERR_INVALID_ARG;
+    if (n_shards == 0 || shard >= n_shards) return PERFT_ERR_INVALID_ARG;
+    if (!board_ok(pos)) return PERFT_ERR_INVALID_ARG;
+    if (split_plies + 1 > depth) split_plies = depth - 1;
+    if (depth - 1 - split_plies > 20) return PERFT_ERR_INVALID_ARG;
+    build_tables();
+    const Board b = from_pos48(pos->bb);
+    const std::vector<u32> mv = legal_moves(b);
+    Frontier f;
+    f.paths.resize(mv.size());
+    for (size_t i = 0; i < mv.size(); i++) f.enumerate((u32)i, make_child(b, mv[i]), split_plies);
+    std::vector<u64> sub;
+    const int rc = frontier_counts(f, depth - 1 - split_plies, shard, n_shards, sub);
+    if (rc != PERFT_OK) return rc;
+    u64 sum = 0;
+    for (size_t i = 0; i < mv.size(); i++) {
+        u64 s = 0;
+        for (const auto &kv : f.paths[i]) s += sub[kv.first] * kv.second;
+        if (moves) move_to_uci(b, mv[i], moves[i]);
+        if (counts) counts[i] = s;
+        sum += s;
+    }
+    if (n_moves) *n_moves = (uint32_t)mv.size();
+    *total = sum;
+    return PERFT_OK;
+}
+
+int perft_deep(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, char (*moves)[6],
+               uint64_t *counts, uint32_t *n_moves, uint64_t *total)
+{
+    return perft_deep_shard(pos, depth, split_plies, 0, 1, moves, counts, n_moves, total);
+}
+
+// Records mode (launcher.h:1579-1695): every line of `in_path` is a FEN
+// followed by an occurrence count; "<line> <perft> <perft x count>" is
+// appended to "<in_path>.op".  Lines already present in the output are
+// skipped, so an interrupted run resumes where it stopped.  Lines are
+// searched in GPU batches of `batch` records.
+int perft_records(const char *in_path, uint32_t depth, uint32_t batch, uint64_t *records_done)
+{
+    if (!in_path || depth > 20) return PERFT_ERR_INVALID_ARG;
+    if (!batch) batch = 4096;
+    FILE *fin = fopen(in_path, "r");
+    if (!fin) return PERFT_ERR_NOT_FOUND;
+    const std::string opPath = std::string(in_path) + ".op";
+    size_t already = 0;
+    if (FILE *fo = fopen(opPath.c_str(), "r")) {
+        char buf[2048];
+        while (fgets(buf, sizeof buf, fo)) already++;
+        fclose(fo);
+    }
+    FILE *fout = fopen(opPath.c_str(), "a");
+    if (!fout) {
+        fclose(fin);
+        return PERFT_ERR_INVALID_ARG;
+    }
+    std::vector<std::string> lines;
+    std::vector<u64> pos, occ;
+    u64 done = 0;
+    int rc = PERFT_OK;
+    auto flush = [&]() -> int {
+        const u32 n = (u32)lines.size();
+        if (!n) return PERFT_OK;
+        std::vector<uint8_t> depths(n, (uint8_t)depth);
+        std::vector<u64> out(n);
+        const int r = engine_batch_host(pos.data(), depths.data(), n, out.data());
+        if (r != PERFT_OK) return r;
+        for (u32 i = 0; i < n; i++)
+            fprintf(fout, "%s %llu %llu\n", lines[i].c_str(), (unsigned long long)out[i],
+                    (unsigned long long)(out[i] * occ[i]));
+        fflush(fout);
+        done += n;
+        lines.clear();
+        pos.clear();
+        occ.clear();
+        return PERFT_OK;
+    };
+    char line[2048];
+    size_t idx = 0;
+    while (fgets(line, sizeof line, fin)) {
+        size_t len = strlen(line);
+        while (len && (line[len - 1] == '\n' || line[len - 1] == '\r')) line[--len] = 0;
+        if (!len) continue;
+        if (idx++ < already) continue;
+        const char *sp = strrchr(line, ' ');
+        const u64 count = sp ? strtoull(sp + 1, nullptr, 10) : 1;
+        perft_pos48 p;
+        if (perft_fen_to_pos(line, &p) != PERFT_OK) {
+            rc = PERFT_ERR_BAD_FEN;
+            break;
+        }
+        lines.emplace_back(line);
+        pos.insert(pos.end(), p.bb, p.bb + 6);
+        occ.push_back(count);
+        if (lines.size() == batch && (rc = flush()) != PERFT_OK) break;
+    }
+    if (rc == PERFT_OK) rc = flush();
+    fclose(fin);
+    fclose(fout);
+    if (records_done) *records_done = done;
+    return rc;
 }
 
 // Feature bits of a position used to stratify synthetic workloads:
