@@ -40,6 +40,7 @@ extern "C" {
 #define PERFT_ERR_ILLEGAL_MOVE    -8
 #define PERFT_ERR_TIMEOUT         -9
 #define PERFT_ERR_NOT_FOUND      -10
+#define PERFT_ERR_IO             -11
 
 /* ---------------------------------------------------------------- types */
 
@@ -169,6 +170,20 @@ int perft_deep(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, cha
 int perft_deep_shard(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, uint32_t shard,
                      uint32_t n_shards, char (*moves)[6], uint64_t *counts, uint32_t *n_moves,
                      uint64_t *total);
+
+/* Result store for deep runs: the counts of completed frontier subtrees,
+ * keyed by the exact board and remaining depth.  perft_deep / perft_deep_shard
+ * look every frontier board up before searching it and add what they search.
+ * With a path, every completed GPU batch is appended to that file (64-byte
+ * checksummed records after a 64-byte header) and flushed, so a run that is
+ * stopped and started again with the same file skips the finished subtrees:
+ * the checkpoint/resume role of the reference's disk hash (launcher.h:699-790,
+ * perfthash.dat).  A torn last record is dropped on open.  A NULL path keeps
+ * the store in host memory only (the reference's complete TT,
+ * launcher.h:585-697). */
+int perft_result_store_open(const char *path);
+int perft_result_store_close(void);
+int perft_result_store_stats(uint64_t *entries, uint64_t *hits, uint64_t *appended);
 
 /* Records mode (launcher.h:1579-1695): each line of in_path is a FEN ending
  * with an occurrence count; "<line> <perft> <perft*count>" is appended to

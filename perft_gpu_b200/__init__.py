@@ -14,7 +14,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from typing import Iterable, List, Sequence
+from typing import Iterable, List, Optional, Sequence
 
 import numpy as np
 
@@ -34,6 +34,7 @@ PERFT_ERR_NO_DEVICE = -7
 PERFT_ERR_ILLEGAL_MOVE = -8
 PERFT_ERR_TIMEOUT = -9
 PERFT_ERR_NOT_FOUND = -10
+PERFT_ERR_IO = -11
 
 SLIDERS_AUTO = -1
 SLIDERS_KOGGE = 0
@@ -149,6 +150,9 @@ def _load():
                                       P(ctypes.c_uint32), u64p]),
         "perft_deep_shard": (ctypes.c_int, [P(_Pos48), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                             ctypes.c_uint32, ctypes.c_void_p, u64p, P(ctypes.c_uint32), u64p]),
+        "perft_result_store_open": (ctypes.c_int, [ctypes.c_char_p]),
+        "perft_result_store_close": (ctypes.c_int, []),
+        "perft_result_store_stats": (ctypes.c_int, [u64p, u64p, u64p]),
         "perft_records": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, u64p]),
     }
     for name, (res, args) in sig.items():
@@ -283,6 +287,22 @@ def deep(pos, depth: int, split_plies: int = 2, shard: int = 0, n_shards: int = 
     raw = bytes(moves)
     div = {raw[6 * i:6 * i + 6].split(b"\0")[0].decode(): int(counts[i]) for i in range(n.value)}
     return int(total.value), div
+
+
+def store_open(path: Optional[str] = None) -> None:
+    """Opens the deep-run result store (file-backed, or host memory for None)."""
+    _check(lib().perft_result_store_open(path.encode() if path else None), "perft_result_store_open")
+
+
+def store_close() -> None:
+    _check(lib().perft_result_store_close(), "perft_result_store_close")
+
+
+def store_stats() -> dict:
+    e, h, a = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_uint64(0)
+    _check(lib().perft_result_store_stats(ctypes.byref(e), ctypes.byref(h), ctypes.byref(a)),
+           "perft_result_store_stats")
+    return {"entries": int(e.value), "hits": int(h.value), "appended": int(a.value)}
 
 
 def records(path: str, depth: int, batch: int = 4096) -> int:

@@ -9,6 +9,8 @@
 //       is accepted for command-line compatibility; one process drives one
 //       GPU (CUDA_VISIBLE_DEVICES / PERFT_DEVICE pick it).  <launchdepth> is
 //       accepted and ignored: level sizes are planned from measured counts.
+//       With PERFT_STORE=<file> the subtrees finished by a deep run are kept
+//       in that file, and a stopped run started again skips them.
 //   perft_gpu --records <file> [<depth>]
 //       Records mode (launcher.h:1579-1695): "<line> <perft> <perft*count>"
 //       per input line appended to <file>.op, resuming after the lines
@@ -44,6 +46,14 @@ int ensure_init()
     if (rc != PERFT_OK) {
         fprintf(stderr, "perft_init failed: %s\n", perft_status_string(rc));
         return rc;
+    }
+    if (const char *st = getenv("PERFT_STORE")) {
+        const int src = perft_result_store_open(st);
+        if (src != PERFT_OK) {
+            fprintf(stderr, "cannot open result store %s: %s\n", st, perft_status_string(src));
+            perft_shutdown();
+            return src;
+        }
     }
     g_ready = true;
     return PERFT_OK;

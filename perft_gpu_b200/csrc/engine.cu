@@ -1706,6 +1706,7 @@ const char *perft_status_string(int status)
     case PERFT_ERR_ILLEGAL_MOVE: return "illegal move";
     case PERFT_ERR_TIMEOUT: return "timed out";
     case PERFT_ERR_NOT_FOUND: return "not found";
+    case PERFT_ERR_IO: return "file I/O error";
     default: return "unknown status";
     }
 }

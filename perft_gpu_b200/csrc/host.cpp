@@ -3,6 +3,7 @@
 // of the move generator for move lists only; every leaf count is computed by
 // the GPU engine (engine.cu).
 #include <algorithm>
+#include <mutex>
 #include <random>
 #include <string>
 #include <unordered_map>
@@ -11,6 +12,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #include "../../include/perft_b200.h"
 #include "movegen.cuh"
@@ -111,6 +113,88 @@ struct Frontier {
     }
 };
 
+// Counts of completed subtrees by (board, remaining depth), optionally backed
+// by an append-only file.  Record: six board words (side bit cleared), the
+// count, the depth and a check word over all of them; 64 bytes.
+struct StoreRecord {
+    u64 w[6];
+    u64 count;
+    u32 depth;
+    u32 check;
+};
+static_assert(sizeof(StoreRecord) == 64, "store record is 64 bytes");
+const char STORE_MAGIC[16] = "PERFTB200STORE1";
+
+u32 record_check(const StoreRecord &r)
+{
+    u64 h = 0x243F6A8885A308D3ULL ^ r.depth;
+    for (u64 x : r.w) h = (h ^ x) * 0x9E3779B97F4A7C15ULL;
+    h = (h ^ r.count) * 0xD6E8FEB86659FD93ULL;
+    h ^= h >> 32;
+    return (u32)h ^ 0xA5A5A5A5u;
+}
+
+struct StoreKey {
+    BoardKey b;
+    u32 depth;
+    bool operator==(const StoreKey &o) const { return depth == o.depth && b == o.b; }
+};
+struct StoreKeyHash {
+    size_t operator()(const StoreKey &k) const { return BoardKeyHash()(k.b) ^ (k.depth * 0x9E3779B97F4A7C15ULL); }
+};
+
+struct ResultStore {
+    std::mutex mu;
+    bool open = false;
+    FILE *f = nullptr;
+    std::unordered_map<StoreKey, u64, StoreKeyHash> map;
+    u64 hits = 0, appended = 0;
+};
+ResultStore g_store;
+
+// Looks up every board of `ids` at `depth`; found ones go to counts and are
+// removed from ids.
+void store_lookup(const Frontier &f, u32 depth, std::vector<u32> &ids, std::vector<u64> &counts)
+{
+    std::lock_guard<std::mutex> lk(g_store.mu);
+    if (!g_store.open) return;
+    size_t k = 0;
+    for (u32 id : ids) {
+        auto it = g_store.map.find(StoreKey{f.boards[id], depth});
+        if (it != g_store.map.end()) {
+            counts[id] = it->second;
+            g_store.hits++;
+        } else {
+            ids[k++] = id;
+        }
+    }
+    ids.resize(k);
+}
+
+int store_add(const Frontier &f, u32 depth, const u32 *ids, const u64 *vals, u32 n)
+{
+    std::lock_guard<std::mutex> lk(g_store.mu);
+    if (!g_store.open) return PERFT_OK;
+    std::vector<StoreRecord> recs;
+    recs.reserve(n);
+    for (u32 i = 0; i < n; i++) {
+        const BoardKey &b = f.boards[ids[i]];
+        if (!g_store.map.emplace(StoreKey{b, depth}, vals[i]).second) continue;
+        StoreRecord r;
+        memcpy(r.w, b.w, sizeof r.w);
+        r.count = vals[i];
+        r.depth = depth;
+        r.check = record_check(r);
+        recs.push_back(r);
+    }
+    if (g_store.f && !recs.empty()) {
+        if (fwrite(recs.data(), sizeof(StoreRecord), recs.size(), g_store.f) != recs.size() || fflush(g_store.f))
+            return PERFT_ERR_IO;
+        g_store.appended += recs.size();
+    }
+    return PERFT_OK;
+}
+
 // perft(depth) of the distinct frontier boards whose index is congruent to
 // `shard` modulo `n_shards`, in GPU batches; the others are left at 0.
 int frontier_counts(const Frontier &f, u32 depth, u32 shard, u32 n_shards, std::vector<u64> &counts)
@@ -120,6 +204,7 @@ int frontier_counts(const Frontier &f, u32 depth, u32 shard, u32 n_shards, std::
     counts.assign(total, 0);
     std::vector<u32> ids;
     for (u32 i = shard; i < total; i += n_shards) ids.push_back(i);
+    store_lookup(f, depth, ids, counts);
     std::vector<u64> pos, out;
     std::vector<uint8_t> depths;
     for (size_t lo = 0; lo < ids.size(); lo += CHUNK) {
@@ -135,6 +220,8 @@ int frontier_counts(const Frontier &f, u32 depth, u32 shard, u32 n_shards, std::
         const int rc = engine_batch_host(pos.data(), depths.data(), n, out.data());
         if (rc != PERFT_OK) return rc;
         for (u32 i = 0; i < n; i++) counts[ids[lo + i]] = out[i];
+        const int src = store_add(f, depth, ids.data() + lo, out.data(), n);
+        if (src != PERFT_OK) return src;
     }
     return PERFT_OK;
 }
@@ -382,6 +469,74 @@ int perft_deep(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, cha
                uint64_t *counts, uint32_t *n_moves, uint64_t *total)
 {
     return perft_deep_shard(pos, depth, split_plies, 0, 1, moves, counts, n_moves, total);
+}
+
+int perft_result_store_open(const char *path)
+{
+    std::lock_guard<std::mutex> lk(g_store.mu);
+    if (g_store.f) fclose(g_store.f);
+    g_store.f = nullptr;
+    g_store.map.clear();
+    g_store.hits = g_store.appended = 0;
+    g_store.open = false;
+    if (!path) {
+        g_store.open = true;
+        return PERFT_OK;
+    }
+    FILE *f = fopen(path, "r+b");
+    if (!f) f = fopen(path, "w+b");
+    if (!f) return PERFT_ERR_IO;
+    char head[64];
+    const size_t got = fread(head, 1, sizeof head, f);
+    if (got == 0) {
+        memset(head, 0, sizeof head);
+        memcpy(head, STORE_MAGIC, sizeof STORE_MAGIC);
+        if (fseek(f, 0, SEEK_SET) || fwrite(head, 1, sizeof head, f) != sizeof head || fflush(f)) {
+            fclose(f);
+            return PERFT_ERR_IO;
+        }
+    } else if (got != sizeof head || memcmp(head, STORE_MAGIC, sizeof STORE_MAGIC) != 0) {
+        fclose(f);
+        return PERFT_ERR_IO;
+    }
+    long good = (long)sizeof head;
+    StoreRecord r;
+    while (fread(&r, sizeof r, 1, f) == 1 && record_check(r) == r.check) {
+        BoardKey b;
+        memcpy(b.w, r.w, sizeof b.w);
+        g_store.map[StoreKey{b, r.depth}] = r.count;
+        good += (long)sizeof r;
+    }
+    // drop a torn or corrupt tail so that appends continue after the last good record
+    if (fflush(f) || ftruncate(fileno(f), good) || fseek(f, good, SEEK_SET)) {
+        fclose(f);
+        g_store.map.clear();
+        return PERFT_ERR_IO;
+    }
+    g_store.f = f;
+    g_store.open = true;
+    return PERFT_OK;
+}
+
+int perft_result_store_close(void)
+{
+    std::lock_guard<std::mutex> lk(g_store.mu);
+    int rc = PERFT_OK;
+    if (g_store.f && fclose(g_store.f)) rc = PERFT_ERR_IO;
+    g_store.f = nullptr;
+    g_store.map.clear();
+    g_store.open = false;
+    return rc;
+}
+
+int perft_result_store_stats(uint64_t *entries, uint64_t *hits, uint64_t *appended)
+{
+    std::lock_guard<std::mutex> lk(g_store.mu);
+    if (!g_store.open) return PERFT_ERR_NOT_INITIALIZED;
+    if (entries) *entries = g_store.map.size();
+    if (hits) *hits = g_store.hits;
+    if (appended) *appended = g_store.appended;
+    return PERFT_OK;
 }
 
 // Records mode (launcher.h:1579-1695): every line of `in_path` is a FEN

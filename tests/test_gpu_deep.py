@@ -149,3 +149,36 @@ def test_uci_go_perft(engine, oracle):
             div[m] = int(c)
     assert nodes == oracle.perft(p, 4)
     assert div == engine.divide(p, 4)
+
+
+@pytest.fixture
+def stored(engine):
+    yield engine
+    engine.store_close()
+
+
+def test_store_resume_skips_finished_subtrees(stored, tmp_path, golden):
+    path = str(tmp_path / "deep.store")
+    start = stored.fen_to_pos(stored.START_FEN)
+    want = _by_name(golden, "initial_position")["counts"]["7"]
+    # first run does only half of the frontier (shard 0 of 2), as if stopped midway
+    stored.store_open(path)
+    half, _ = stored.deep(start, 7, 3, shard=0, n_shards=2)
+    first = stored.store_stats()["appended"]
+    assert first > 0
+    stored.store_close()
+    # the resumed run searches only the other half
+    stored.store_open(path)
+    assert stored.store_stats()["entries"] == first
+    total, div = stored.deep(start, 7, 3)
+    st = stored.store_stats()
+    assert total == want and 0 < half < total
+    assert st["hits"] == first and st["appended"] > 0
+    stored.store_close()
+    # a third run finds everything and launches no leaf kernel
+    stored.store_open(path)
+    stored.reset_stats()
+    again, div2 = stored.deep(start, 7, 3)
+    assert again == want and div2 == div
+    assert stored.stats()["leaf_launches"] == 0
+    assert stored.store_stats()["appended"] == 0
