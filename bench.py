@@ -289,7 +289,10 @@ def run_ours(args):
     torch.cuda.synchronize()
     e_start.record()
     for _ in range(args.steps):
-        host_out = pg.perft_batch(host_pos, depths)
+        if args.form == "single":
+            host_out = np.array([pg.perft(host_pos[i], int(depths[i])) for i in range(n)], dtype=np.uint64)
+        else:
+            host_out = pg.perft_batch(host_pos, depths)
     e_end.record()
     torch.cuda.synchronize()
     e_ms = e_start.elapsed_time(e_end)
