@@ -372,13 +372,15 @@ def run_tt(args):
     from perft_gpu_b200 import workloads as W
     pos, depths = W.tt_positions()
     depths = np.minimum(depths, args.max_depth).astype(np.uint8)
-    pg.init(device=0)
+    arena = int(args.arena_gb * (1 << 30))
+    pd = args.parity_depth
+    pg.init(device=0, arena_bytes=arena)
     t0 = time.perf_counter()
-    d8_plain = pg.perft_batch(pos, 8)
+    d8_plain = pg.perft_batch(pos, pd)
     t_plain = time.perf_counter() - t0
-    pg.init(device=0, tt_log2_entries=args.tt_log2)
+    pg.init(device=0, arena_bytes=arena, tt_log2_entries=args.tt_log2)
     t0 = time.perf_counter()
-    d8_tt = pg.perft_batch(pos, 8)
+    d8_tt = pg.perft_batch(pos, pd)
     t_tt8 = time.perf_counter() - t0
     times, counts = [], None
     for step in range(args.warmup + args.steps):
@@ -398,8 +400,8 @@ def run_tt(args):
             "config": {"workload": "4 seeded playouts of 12-24 plies, TT of 2^%d x 16 B, table cleared each step"
                                    % args.tt_log2, "depths": depths.tolist()},
             "counts": [int(x) for x in counts],
-            "parity_depth8": {"equal": bool(np.array_equal(d8_plain, d8_tt)), "no_tt_s": t_plain, "tt_s": t_tt8,
-                              "counts": [int(x) for x in d8_plain]},
+            "parity_depth%d" % pd: {"equal": bool(np.array_equal(d8_plain, d8_tt)), "no_tt_s": t_plain,
+                                    "tt_s": t_tt8, "counts": [int(x) for x in d8_plain]},
             "tt": {k: st[k] for k in ("tt_entries", "tt_probes", "tt_hits", "tt_duplicates", "tt_stores")},
             "timing": "host wall clock around the synchronous perft_batch call"}
     print(json.dumps(line), flush=True)
@@ -463,6 +465,8 @@ def main():
                     help="batch workload: one batched call, or one call per position")
     ap.add_argument("--tt-log2", type=int, default=30, help="tt workload: table entries (log2)")
     ap.add_argument("--max-depth", type=int, default=10, help="tt workload: cap on the depths")
+    ap.add_argument("--parity-depth", type=int, default=8,
+                    help="tt workload: depth of the table vs no-table equality check")
     ap.add_argument("--rate", type=float, default=1000.0, help="serve workload: offered queries/s")
     ap.add_argument("--queries", type=int, default=2000, help="serve workload: trace length")
     ap.add_argument("--serve-memory-gb", type=float, default=120.0, help="serve workload: admission budget")

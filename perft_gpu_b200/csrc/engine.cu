@@ -611,11 +611,19 @@ __device__ __forceinline__ u64 zobrist_rel(const Board &b)
     return h;
 }
 
-// Warp-aggregated increment of a statistics counter.
+// Block-aggregated increment of a statistics counter: warp ballots summed
+// in shared memory, then one global atomic per block.  Per-warp atomics on
+// the same few counters serialised in L2 and cost a large part of the table
+// kernels' time.  Every thread of the block must call it.
 __device__ __forceinline__ void count_stat(unsigned long long *ctr, bool hit)
 {
-    const unsigned m = __ballot_sync(__activemask(), hit);
-    if (m && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(ctr, (unsigned long long)__popc(m));
+    __shared__ unsigned sCount;
+    if (threadIdx.x == 0) sCount = 0;
+    __syncthreads();
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(&sCount, (unsigned)__popc(m));
+    __syncthreads();
+    if (threadIdx.x == 0 && sCount) atomicAdd(ctr, (unsigned long long)sCount);
 }
 
 // Hash every node, probe the table, and insert misses into the level's
