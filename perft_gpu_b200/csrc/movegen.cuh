@@ -565,22 +565,11 @@ PG_HD u32 count_moves_fused(const Board &b)
     const u64 tP = pawns & theirs, tN = b.knights & theirs, tB = b.bq & theirs, tR = b.rq & theirs;
     const u32 st = (u32)(b.pawns & 0xFF);
 
-    const u64 chk = (pawn_att_up(myK) & tP) | (PG_TAB(knight[ksq]) & tN) | (magic_bishop(ksq, occ) & tB) |
-                    (magic_rook(ksq, occ) & tR);
-    u64 cm = ~0ULL, xray = 0;
-    if (chk) {
-        cm = (chk & (chk - 1)) ? 0 : (chk | PG_TAB(between[ksq][ctz(chk)]));
-        u64 sl = chk & (tB | tR);
-        while (sl) {
-            const int c = ctz(sl);
-            sl &= sl - 1;
-            xray |= PG_TAB(line[ksq][c]) & ~PG_TAB(between[ksq][c]) & ~(1ULL << c);
-        }
-    }
-    const bool inCheck = chk != 0;
-
-    // pins: each pinned piece may only move along its pin line
-    u64 pinned = 0;
+    // pins and slider checks: every opponent slider on a line through the
+    // king (a sniper) either checks (nothing between), pins (exactly one own
+    // piece between) or neither; each pinned piece may only move along its
+    // pin line
+    u64 pinned = 0, slChk = 0;
     u32 nPinned = 0;
     u64 snipers = (PG_TAB(rookRays[ksq]) & tR) | (PG_TAB(bishopRays[ksq]) & tB);
     while (snipers) {
@@ -588,7 +577,11 @@ PG_HD u32 count_moves_fused(const Board &b)
         snipers &= snipers - 1;
         const u64 btw = PG_TAB(between[ksq][s]);
         const u64 blk = btw & occ;
-        if (!blk || (blk & (blk - 1)) || !(blk & mine)) continue;
+        if (!blk) {
+            slChk |= 1ULL << s;
+            continue;
+        }
+        if ((blk & (blk - 1)) || !(blk & mine)) continue;
         pinned |= blk;
         const bool diag = (PG_TAB(bishopRays[ksq]) >> s) & 1;
         if (blk & (diag ? b.bq : b.rq)) {
@@ -603,6 +596,18 @@ PG_HD u32 count_moves_fused(const Board &b)
             }
         }
     }
+    const u64 chk = (pawn_att_up(myK) & tP) | (PG_TAB(knight[ksq]) & tN) | slChk;
+    u64 cm = ~0ULL, xray = 0;
+    if (chk) {
+        cm = (chk & (chk - 1)) ? 0 : (chk | PG_TAB(between[ksq][ctz(chk)]));
+        u64 sl = slChk;
+        while (sl) {
+            const int c = ctz(sl);
+            sl &= sl - 1;
+            xray |= PG_TAB(line[ksq][c]) & ~PG_TAB(between[ksq][c]) & ~(1ULL << c);
+        }
+    }
+    const bool inCheck = chk != 0;
     u32 n = inCheck ? 0 : nPinned;  // pinned pieces never resolve a check
     const u64 targets = notMine & cm;
 
