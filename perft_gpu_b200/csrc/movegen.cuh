@@ -45,6 +45,11 @@
 #ifndef PG_KNIGHT_LUT
 #define PG_KNIGHT_LUT 1
 #endif
+// PG_GEN_MAGIC 1: move generation looks up each slider's targets in the
+// magic tables whatever the slider variant.
+#ifndef PG_GEN_MAGIC
+#define PG_GEN_MAGIC 1
+#endif
 
 #ifdef __CUDACC__
 #define PG_HD __host__ __device__ __forceinline__
@@ -842,6 +847,10 @@ PG_HD void emit_pawn(Sink &out, int from, int to, u32 flags)
 template <int SV, class Sink>
 PG_HD void gen_moves(const Board &b, Sink &out)
 {
+    // per-piece targets: one magic lookup per slider beats a single-bit
+    // Kogge-Stone fill in every variant; the variant still decides the
+    // set-wise opponent attack map
+    constexpr int GEN_SV = PG_GEN_MAGIC ? SV_MAGIC : SV;
     Ctx c;
     setup_ctx<SV>(b, c);
     const u64 notMine = ~c.mine;
@@ -877,8 +886,8 @@ PG_HD void gen_moves(const Board &b, Sink &out)
             continue;
         }
         u64 t = 0;
-        if (p & b.bq) t |= bishop_att<SV>(s, c.occ);
-        if (p & b.rq) t |= rook_att<SV>(s, c.occ);
+        if (p & b.bq) t |= bishop_att<GEN_SV>(s, c.occ);
+        if (p & b.rq) t |= rook_att<GEN_SV>(s, c.occ);
         emit_targets(out, s, t & notMine & line);
     }
 
@@ -893,13 +902,13 @@ PG_HD void gen_moves(const Board &b, Sink &out)
     while (B) {
         const int s = ctz(B);
         B &= B - 1;
-        emit_targets(out, s, bishop_att<SV>(s, c.occ) & targets);
+        emit_targets(out, s, bishop_att<GEN_SV>(s, c.occ) & targets);
     }
     u64 R = b.rq & c.mine & ~pinned;
     while (R) {
         const int s = ctz(R);
         R &= R - 1;
-        emit_targets(out, s, rook_att<SV>(s, c.occ) & targets);
+        emit_targets(out, s, rook_att<GEN_SV>(s, c.occ) & targets);
     }
     const u64 P = c.pawns & c.mine & ~pinned;
     const u64 p1 = sh_n(P) & c.empty;
