@@ -416,7 +416,7 @@ def run_serve(args):
     from perft_gpu_b200 import workloads as W
     pos, depths, arrivals = W.serving_trace(n=args.queries, rate_qps=args.rate, seed=5)
     pg.init(device=0)
-    pg.serve_start(memory_bytes=int(args.serve_memory_gb * (1 << 30)))
+    pg.serve_start(memory_bytes=int(args.serve_memory_gb * (1 << 30)), step_items=args.serve_step_items)
     tickets = [None] * len(pos)
     t_start = time.perf_counter()
     for i in range(len(pos)):
@@ -438,7 +438,8 @@ def run_serve(args):
             "n_gpus": 1, "higher_is_better": True, "data": "synthetic", "dtype": "u64",
             "config": {"workload": "Poisson arrivals, seeded 0-40-ply positions, depth U[3,7]",
                        "offered_rate_qps": args.rate, "queries": len(pos),
-                       "memory_budget_gb": args.serve_memory_gb or "90% of free arena"},
+                       "memory_budget_gb": args.serve_memory_gb or "90% of free arena",
+                       "step_items": args.serve_step_items or "server default"},
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "max": float(lat.max())},
             "leaf_nodes_per_s": float(counts.sum()) / wall,
@@ -470,6 +471,8 @@ def main():
     ap.add_argument("--rate", type=float, default=1000.0, help="serve workload: offered queries/s")
     ap.add_argument("--queries", type=int, default=2000, help="serve workload: trace length")
     ap.add_argument("--serve-memory-gb", type=float, default=120.0, help="serve workload: admission budget")
+    ap.add_argument("--serve-step-items", type=int, default=0,
+                    help="serve workload: items per level per scheduler step (0 = server default)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -160,3 +160,20 @@ def test_small_arena_chunks_levels(engine, golden):
         assert engine.stats()["chunked_levels"] > 0
     finally:
         engine.init(device=0, arena_bytes=8 << 30)
+
+
+def test_many_move_positions(engine, oracle):
+    """94-170 legal moves per node (and the colour mirrors): single calls,
+    one batch and every slider variant against the oracle."""
+    from tests._positions import many_moves_with_mirrors
+    pos = [engine.fen_to_pos(f) for f in many_moves_with_mirrors()]
+    want = {d: [oracle.perft(p, d) for p in pos] for d in (1, 2, 3)}
+    for d in (1, 2, 3):
+        assert [engine.perft(p, d) for p in pos] == want[d]
+        assert [int(x) for x in engine.perft_batch(pos, d)] == want[d]
+    for v in range(5):
+        engine.init(device=0, arena_bytes=8 << 30, sliders_expand=v, sliders_leaf=v)
+        assert [int(x) for x in engine.perft_batch(pos, 3)] == want[3], v
+    engine.init(device=0, arena_bytes=8 << 30)
+    d4 = engine.perft_batch(pos[:2], 4)
+    assert [int(x) for x in d4] == [oracle.perft(p, 4) for p in pos[:2]]

@@ -108,3 +108,21 @@ def test_opcount_build_and_work_figures():
     res = json.loads(out)
     assert res["leaves"] == 197281
     assert abs(res["c_count"] - wf["start"]["c_count"]) < 1e-6
+
+
+@needs_ref
+def test_oracle_vs_reference_many_moves(oracle):
+    """Crafted 94-170-move positions and their colour mirrors: the oracle,
+    the reference's host perft and the mirror all agree."""
+    from tests._positions import MANY_MOVES, mirror_fen
+    for fen in MANY_MOVES:
+        counts = []
+        for f in (fen, mirror_fen(fen)):
+            p = P6()
+            assert ref.ref_fen_to_pos(f.encode(), p) == 0, f
+            arr = np.array(list(p), dtype=np.uint64)
+            c = [ref.ref_perft(p, d) for d in (1, 2, 3)]
+            assert [oracle.perft(arr, d) for d in (1, 2, 3)] == c, f
+            counts.append(c)
+        assert counts[0] == counts[1], fen
+        assert counts[0][0] >= 94
