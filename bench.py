@@ -177,7 +177,7 @@ def cpu_sample(pos, depths, budget_s, expected=None, threads=None):
     order = np.random.default_rng(123).permutation(len(pos))
     done, leaves, t0 = 0, 0, time.perf_counter()
     mismatches = 0
-    group = max(1, min(64, len(pos)))
+    group = max(1, min(4, len(pos)))  # doubles up to 128: short budgets stop early
     while done < len(pos) and time.perf_counter() - t0 < budget_s:
         idx = order[done:done + group]
         p = np.ascontiguousarray(pos[idx], dtype=np.uint64)
