@@ -45,6 +45,11 @@
 #ifndef PG_KNIGHT_LUT
 #define PG_KNIGHT_LUT 1
 #endif
+// PG_KS_LINE 1: the fused count fills both directions of a line from one
+// propagator chain.
+#ifndef PG_KS_LINE
+#define PG_KS_LINE 1
+#endif
 // PG_GEN_MAGIC 1: move generation looks up each slider's targets in the
 // magic tables whatever the slider variant.
 #ifndef PG_GEN_MAGIC
@@ -511,6 +516,43 @@ PG_HD void ks_pair(u64 eGen, u64 oGen, u64 empty, u64 wrap, u64 targets, u64 &at
     }
 }
 
+// Both directions of one line (up by S and down by S) for the two generator
+// sets, from one propagator chain: the down-direction propagators are the
+// up-direction ones shifted down (P & P>>S == (P & P<<S) >> S, and the
+// second doubling step shifts by 3S).  For diagonals, p0 excludes files a
+// and h for both directions: a diagonal ray only enters the file it moves
+// towards as its last square, which the final step adds, and never enters
+// the other one without wrapping.  wrapUp / wrapDown mask the final step.
+template <int S, int MODE>
+PG_HD void ks_line(u64 eGen, u64 oGen, u64 p0, u64 wrapUp, u64 wrapDown, u64 targets, u64 &attacked, u32 &n)
+{
+    const u64 p1 = p0 & shl<S, MODE>(p0);
+    const u64 p2 = p1 & shl<2 * S, MODE>(p1);
+    {
+        u64 e = eGen, o = oGen;
+        e |= p0 & shl<S, MODE>(e);
+        o |= p0 & shl<S, MODE>(o);
+        e |= p1 & shl<2 * S, MODE>(e);
+        o |= p1 & shl<2 * S, MODE>(o);
+        e |= p2 & shl<4 * S, MODE>(e);
+        o |= p2 & shl<4 * S, MODE>(o);
+        attacked |= shl<S, MODE>(e) & wrapUp;
+        n += popc(shl<S, MODE>(o) & wrapUp & targets);
+    }
+    {
+        const u64 q1 = shr<S, MODE>(p1), q2 = shr<3 * S, MODE>(p2);
+        u64 e = eGen, o = oGen;
+        e |= p0 & shr<S, MODE>(e);
+        o |= p0 & shr<S, MODE>(o);
+        e |= q1 & shr<2 * S, MODE>(e);
+        o |= q1 & shr<2 * S, MODE>(o);
+        e |= q2 & shr<4 * S, MODE>(e);
+        o |= q2 & shr<4 * S, MODE>(o);
+        attacked |= shr<S, MODE>(e) & wrapDown;
+        n += popc(shr<S, MODE>(o) & wrapDown & targets);
+    }
+}
+
 // 64-bit bit reversal (file h <-> a, rank 8 <-> 1 mirrored together).
 PG_HD u64 brev64(u64 x)
 {
@@ -632,8 +674,12 @@ PG_HD u32 count_moves_fused(const Board &b)
             x &= x - 1;
         }
     } else {
+#if PG_KS_LINE
+        ks_line<8, M>(tR, R, empty, ~0ULL, ~0ULL, targets, attacked, n);
+#else
         ks_pair<8, true, M>(tR, R, empty, ~0ULL, targets, attacked, n);
         ks_pair<8, false, M>(tR, R, empty, ~0ULL, targets, attacked, n);
+#endif
         if (PG_RANK_SUB) {
             rank_pair<false>(tR, R, occ | FILEA, targets, attacked, n);
             rank_pair<true>(tR, R, brev64(occ) | FILEA, targets, attacked, n);
@@ -641,10 +687,16 @@ PG_HD u32 count_moves_fused(const Board &b)
             ks_pair<1, true, M>(tR, R, empty, ~FILEA, targets, attacked, n);
             ks_pair<1, false, M>(tR, R, empty, ~FILEH, targets, attacked, n);
         }
+#if PG_KS_LINE
+        const u64 inner = empty & ~(FILEA | FILEH);
+        ks_line<9, M>(tB, B, inner, ~FILEA, ~FILEH, targets, attacked, n);  // north-east, south-west
+        ks_line<7, M>(tB, B, inner, ~FILEH, ~FILEA, targets, attacked, n);  // north-west, south-east
+#else
         ks_pair<9, true, M>(tB, B, empty, ~FILEA, targets, attacked, n);
         ks_pair<7, true, M>(tB, B, empty, ~FILEH, targets, attacked, n);
         ks_pair<7, false, M>(tB, B, empty, ~FILEA, targets, attacked, n);
         ks_pair<9, false, M>(tB, B, empty, ~FILEH, targets, attacked, n);
+#endif
     }
     attacked |= pawn_att_down(tP) | knight_set_att(tN) | PG_TAB(king[ctz(b.kings & theirs)]);
 
