@@ -166,6 +166,24 @@ PG_HD int popc(u64 x)
 #endif
 }
 
+// Popcount of the high byte (the eighth rank) and of the low word (ranks 1-4).
+PG_HD int popc_byte7(u64 x)
+{
+#ifdef __CUDA_ARCH__
+    return __popc((u32)(x >> 56));
+#else
+    return __builtin_popcount((unsigned)(x >> 56));
+#endif
+}
+PG_HD int popc_lo(u64 x)
+{
+#ifdef __CUDA_ARCH__
+    return __popc((u32)x);
+#else
+    return __builtin_popcount((unsigned)x);
+#endif
+}
+
 PG_HD int ctz(u64 x)
 {
 #ifdef __CUDA_ARCH__
@@ -714,11 +732,14 @@ PG_HD u32 count_moves_fused(const Board &b)
     const u64 P = pawns & mine & ~pinned;
     const u64 p1 = sh_n(P) & empty;
     const u64 p1c = p1 & cm;
-    n += popc(p1c) + 3 * popc(p1c & RANK8);
-    n += popc(sh_n(p1 & RANK3) & empty & cm);
+    n += popc_lo(sh_n(p1 & RANK3) & empty & cm);  // double pushes land on the fourth rank
     const u64 capT = theirs & cm;
     const u64 cl = sh_nw(P) & capT, cr = sh_ne(P) & capT;
-    n += popc(cl) + popc(cr) + 3 * (popc(cl & RANK8) + popc(cr & RANK8));
+    // pushes land on empty squares and captures on occupied ones, so the push
+    // and left-capture sets are disjoint and share one popcount; promotions
+    // (the eighth rank, the high byte) add three more moves each
+    const u64 pl = p1c | cl;
+    n += popc(pl) + popc(cr) + 3 * (popc_byte7(pl) + popc_byte7(cr));
 
     // en passant: out of check, or capturing the checking pawn
     const u32 epf = st >> 4;
