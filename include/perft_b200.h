@@ -67,7 +67,7 @@ typedef struct perft_config {
     int      sliders_expand;  /* PERFT_SLIDERS_* for interior plies */
     int      sliders_leaf;    /* PERFT_SLIDERS_* for the count-only last ply */
     int      tt_log2_entries; /* transposition table size; 0 = no table */
-    uint64_t zobrist_seed;    /* seed of the 781 Zobrist keys (TT only) */
+    uint64_t zobrist_seed;    /* seed of the two sets of 781 Zobrist keys (TT only) */
 } perft_config;
 
 /* Defaults: device 0, automatic arena, autotuned sliders, no TT. */

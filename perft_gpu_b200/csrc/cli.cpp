@@ -42,6 +42,7 @@ int ensure_init()
     if (const char *d = getenv("PERFT_DEVICE")) cfg.device = atoi(d);
     if (const char *a = getenv("PERFT_ARENA_GB")) cfg.arena_bytes = (uint64_t)(atof(a) * (1ull << 30));
     if (const char *t = getenv("PERFT_TT_LOG2")) cfg.tt_log2_entries = (uint32_t)atoi(t);
+    if (const char *z = getenv("PERFT_ZOBRIST_SEED")) cfg.zobrist_seed = strtoull(z, nullptr, 0);
     const int rc = perft_init(&cfg);
     if (rc != PERFT_OK) {
         fprintf(stderr, "perft_init failed: %s\n", perft_status_string(rc));

@@ -563,16 +563,22 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
 }
 
 // ====================================================== transposition table
-// Lockless table of 16-byte entries {key ^ value, value}: a torn or foreign
-// entry fails the XOR check (the reference's scheme, perft_bb.h:759-764,
-// with 64-bit keys).  Keys are Zobrist hashes of the side-relative board
-// (781 seeded keys: 12 piece kinds x 64 squares, 4 castling rights, 8
-// en-passant files, one spare) XOR a per-remaining-depth key, so one table
-// holds every depth ("per-depth slots").  Perft is invariant under the
+// Lockless table of 16-byte entries {verify ^ value, value} at the slot the
+// slot key picks: a torn or foreign entry fails the XOR check (the
+// reference's scheme, perft_bb.h:759-764, whose 128-bit hash is here two
+// independent 64-bit hashes).  Both are Zobrist hashes of the side-relative
+// board (two sets of 781 seeded keys: 12 piece kinds x 64 squares, 4 castling
+// rights, 8 en-passant files, one spare) XOR a per-remaining-depth key, so
+// one table holds every depth ("per-depth slots").  Perft is invariant under the
 // colour mirror, so a position and its mirror may share an entry.
 constexpr int ZOB_KEYS = 781;
 constexpr int ZOB_DEPTH_KEYS = 32;
-__device__ u64 d_zobrist[ZOB_KEYS + ZOB_DEPTH_KEYS];
+// Two independent key sets (x, y): the x hash picks the table slot and the
+// de-duplication slot, the y hash verifies.  A verification key that shares
+// no bits with the index keeps false hits at 2^-64 per probe; with one 64-bit
+// hash doing both, only the bits above the index are checked, and searches
+// with ~1e12 probes (perft 12 of the initial position) did see false hits.
+__device__ ulonglong2 d_zobrist[ZOB_KEYS + ZOB_DEPTH_KEYS];
 
 constexpr u32 ALIAS_HIT = 0xFFFFFFFFu;     // value came from the table
 constexpr u32 ALIAS_NOSLOT = 0xFFFFFFFEu;  // not de-duplicated (set full)
@@ -583,31 +589,39 @@ struct TTStats {
     unsigned long long probes, hits, aliases, stores;
 };
 
-__device__ __forceinline__ u64 zobrist_rel(const Board &b)
+__device__ __forceinline__ void zx(ulonglong2 &h, int k)
+{
+    const ulonglong2 z = __ldg(&d_zobrist[k]);
+    h.x ^= z.x;
+    h.y ^= z.y;
+}
+
+// Both Zobrist hashes of a side-relative board (one 16-byte key load per piece).
+__device__ __forceinline__ ulonglong2 zobrist_rel(const Board &b)
 {
     const u64 pawns = b.pawns & RANKS2TO7;
     const u64 occ = pawns | b.knights | b.bq | b.rq | b.kings;
     const u64 theirs = occ ^ b.mine;
     const u64 sets[6] = {pawns, b.knights, b.bq & ~b.rq, b.rq & ~b.bq, b.bq & b.rq, b.kings};
-    u64 h = 0;
+    ulonglong2 h = make_ulonglong2(0, 0);
 #pragma unroll
     for (int pc = 0; pc < 6; pc++) {
         u64 m = sets[pc] & b.mine;
         while (m) {
-            h ^= __ldg(&d_zobrist[pc * 64 + ctz(m)]);
+            zx(h, pc * 64 + ctz(m));
             m &= m - 1;
         }
         u64 t = sets[pc] & theirs;
         while (t) {
-            h ^= __ldg(&d_zobrist[(6 + pc) * 64 + ctz(t)]);
+            zx(h, (6 + pc) * 64 + ctz(t));
             t &= t - 1;
         }
     }
     const u32 st = (u32)(b.pawns & 0xFF);
 #pragma unroll
     for (int k = 0; k < 4; k++)
-        if (st & (1u << k)) h ^= __ldg(&d_zobrist[768 + k]);
-    if (st >> 4) h ^= __ldg(&d_zobrist[772 + (st >> 4) - 1]);
+        if (st & (1u << k)) zx(h, 768 + k);
+    if (st >> 4) zx(h, 772 + (st >> 4) - 1);
     return h;
 }
 
@@ -630,7 +644,8 @@ __device__ __forceinline__ void count_stat(unsigned long long *ctr, bool hit)
 // de-duplication set (lowest index wins).  Hits get their value and no
 // children; their alias is ALIAS_HIT.  Misses keep the set slot in alias.
 __global__ void __launch_bounds__(256) k_tt_probe(const u64 *__restrict__ planes, u64 stride, u64 n, int remaining,
-                                                  bool probe, u32 *__restrict__ cnt, u64 *__restrict__ hash,
+                                                  bool probe, u64 keyMask, u32 *__restrict__ cnt,
+                                                  u64 *__restrict__ hash, u64 *__restrict__ hash2,
                                                   unsigned long long *__restrict__ acc, u32 *__restrict__ alias,
                                                   const ulonglong2 *tt, u64 ttMask, u64 *__restrict__ dkey,
                                                   u32 *__restrict__ downer, u64 dMask, TTStats *ts)
@@ -640,12 +655,16 @@ __global__ void __launch_bounds__(256) k_tt_probe(const u64 *__restrict__ planes
     if (i < n) {
         const Board b{planes[i], planes[stride + i], planes[2 * stride + i], planes[3 * stride + i],
                       planes[4 * stride + i], planes[5 * stride + i]};
-        const u64 h = zobrist_rel(b) ^ __ldg(&d_zobrist[ZOB_KEYS + remaining]);
+        ulonglong2 z = zobrist_rel(b);
+        zx(z, ZOB_KEYS + remaining);
+        const u64 h = z.x & keyMask;  // slot key (table index, de-duplication set)
+        const u64 g = z.y;            // verification key
         hash[i] = h;
+        hash2[i] = g;
         acc[i] = 0;
         if (probe) {
             const ulonglong2 e = tt[h & ttMask];
-            if ((e.x ^ e.y) == h) {
+            if ((e.x ^ e.y) == g) {
                 hit = true;
                 acc[i] = e.y;
                 cnt[i] = 0;
@@ -677,9 +696,12 @@ __global__ void __launch_bounds__(256) k_tt_probe(const u64 *__restrict__ planes
     }
 }
 
-// Turns set slots into owner indices; duplicates lose their children.
+// Turns set slots into owner indices; duplicates lose their children.  A
+// node shares its owner's slot key; it is a duplicate only if the
+// verification keys match too, otherwise it is searched on its own.
 __global__ void __launch_bounds__(256) k_tt_dedup(u64 n, u32 *__restrict__ cnt, u32 *__restrict__ alias,
-                                                  const u32 *__restrict__ downer, TTStats *ts)
+                                                  const u32 *__restrict__ downer, const u64 *__restrict__ hash2,
+                                                  TTStats *ts)
 {
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     bool dup = false;
@@ -687,10 +709,14 @@ __global__ void __launch_bounds__(256) k_tt_dedup(u64 n, u32 *__restrict__ cnt, 
         const u32 a = alias[i];
         if (a != ALIAS_HIT && a != ALIAS_NOSLOT) {
             const u32 o = downer[a];
-            alias[i] = o;
-            if (o != (u32)i) {
+            if (o == (u32)i) {
+                alias[i] = o;
+            } else if (hash2[o] == hash2[i]) {
+                alias[i] = o;
                 cnt[i] = 0;
                 dup = true;
+            } else {
+                alias[i] = ALIAS_NOSLOT;
             }
         }
     }
@@ -702,6 +728,7 @@ __global__ void __launch_bounds__(256) k_tt_dedup(u64 n, u32 *__restrict__ cnt, 
 // parent level (nodes are ordered by parent: segmented warp sums, then one
 // atomic per parent run).  At level 0 the values go to the roots' results.
 __global__ void __launch_bounds__(256) k_tt_finish(u64 n, bool store, const u64 *__restrict__ hash,
+                                                   const u64 *__restrict__ hash2,
                                                    unsigned long long *__restrict__ acc, const u32 *__restrict__ alias,
                                                    const u32 *__restrict__ parent, unsigned long long *parentAcc,
                                                    ulonglong2 *tt, u64 ttMask, TTStats *ts)
@@ -717,7 +744,7 @@ __global__ void __launch_bounds__(256) k_tt_finish(u64 n, bool store, const u64 
         if (a != ALIAS_HIT && a != ALIAS_NOSLOT && a != (u32)i) {
             v = acc[a];  // the owner is final: its subtree finished before this kernel
         } else if (a != ALIAS_HIT && store) {
-            tt[hash[i] & ttMask] = make_ulonglong2(hash[i] ^ v, v);
+            tt[hash[i] & ttMask] = make_ulonglong2(hash2[i] ^ v, v);
             stored = true;
         }
         key = parent[i];
@@ -755,15 +782,16 @@ struct DeviceLevel {
     u32 *root;  // root id (no TT) or parent index in the previous level (TT)
     u64 n;
     // transposition-table runs only
-    u64 *hash = nullptr;
+    u64 *hash = nullptr;   // slot key
+    u64 *hash2 = nullptr;  // verification key
     unsigned long long *acc = nullptr;  // perft of each node's subtree
     u32 *alias = nullptr;               // owner index, ALIAS_HIT or ALIAS_NOSLOT
 };
 
-// Bytes of one TT level node: the plain node plus hash, subtree sum, alias,
+// Bytes of one TT level node: the plain node plus two hashes, subtree sum, alias,
 // and the transient de-duplication set (at most 2.5 slots of 12 bytes per
 // node; it is released before the scan, so this over-counts slightly).
-constexpr u64 NODE_BYTES_TT = NODE_BYTES + 8 + 8 + 4 + 30;
+constexpr u64 NODE_BYTES_TT = NODE_BYTES + 8 + 8 + 8 + 4 + 30;
 
 class Engine {
 public:
@@ -848,6 +876,7 @@ public:
 private:
     ulonglong2 *tt = nullptr;
     u64 ttMask = 0;
+    u64 ttKeyMask = ~0ULL;
     TTStats *dTTStats = nullptr;
     int ttMinDepth = 2;
     int check(cudaError_t e, const char *what);
@@ -962,16 +991,26 @@ int Engine::init(const perft_config &cfg)
 
     // Zobrist keys (splitmix64 of the seed) and the transposition table
     {
-        u64 keys[ZOB_KEYS + ZOB_DEPTH_KEYS];
+        ulonglong2 keys[ZOB_KEYS + ZOB_DEPTH_KEYS];
         u64 x = cfg.zobrist_seed;
-        for (int k = 0; k < ZOB_KEYS + ZOB_DEPTH_KEYS; k++) {
+        auto next = [&x]() {
             x += 0x9E3779B97F4A7C15ULL;
             u64 z = x;
             z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
             z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-            keys[k] = z ^ (z >> 31);
-        }
+            return z ^ (z >> 31);
+        };
+        for (int k = 0; k < ZOB_KEYS + ZOB_DEPTH_KEYS; k++) keys[k].x = next();
+        for (int k = 0; k < ZOB_KEYS + ZOB_DEPTH_KEYS; k++) keys[k].y = next();
         ENG_TRY(cudaMemcpyToSymbol(d_zobrist, keys, sizeof keys));
+        // PERFT_TT_INDEX_KEY_BITS=b keeps only the low b bits of the slot key:
+        // a test setting that makes different positions share table and
+        // de-duplication slots, which the verification key must then tell apart
+        ttKeyMask = ~0ULL;
+        if (const char *kb = getenv("PERFT_TT_INDEX_KEY_BITS")) {
+            const int bits = atoi(kb);
+            if (bits >= 1 && bits < 64) ttKeyMask = (1ULL << bits) - 1;
+        }
     }
     ENG_TRY(cudaMalloc(&dTTStats, sizeof(TTStats)));
     ENG_TRY(cudaMemset(dTTStats, 0, sizeof(TTStats)));
@@ -1255,9 +1294,10 @@ bool Engine::alloc_level_tt(DeviceLevel &L, u64 n)
 {
     if (!alloc_level(L, n)) return false;
     L.hash = (u64 *)alloc(8 * L.stride);
+    L.hash2 = (u64 *)alloc(8 * L.stride);
     L.acc = (unsigned long long *)alloc(8 * L.stride);
     L.alias = (u32 *)alloc(4 * L.stride);
-    return L.hash && L.acc && L.alias;
+    return L.hash && L.hash2 && L.acc && L.alias;
 }
 
 int Engine::tt_clear()
@@ -1289,9 +1329,10 @@ int Engine::process_level_tt(const DeviceLevel &L, int remaining, unsigned long 
     if (!dkey || !downer) return PERFT_ERR_OUT_OF_MEMORY;
     ENG_TRY(cudaMemsetAsync(dkey, 0xFF, 8 * dsize, stream));
     ENG_TRY(cudaMemsetAsync(downer, 0xFF, 4 * dsize, stream));
-    k_tt_probe<<<nb, 256, 0, stream>>>(L.planes, L.stride, L.n, remaining, useTT, L.cnt, L.hash, L.acc, L.alias,
+    k_tt_probe<<<nb, 256, 0, stream>>>(L.planes, L.stride, L.n, remaining, useTT, ttKeyMask, L.cnt, L.hash, L.hash2,
+                                       L.acc, L.alias,
                                        tt, ttMask, dkey, downer, dsize - 1, dTTStats);
-    k_tt_dedup<<<nb, 256, 0, stream>>>(L.n, L.cnt, L.alias, downer, dTTStats);
+    k_tt_dedup<<<nb, 256, 0, stream>>>(L.n, L.cnt, L.alias, downer, L.hash2, dTTStats);
     stats.other_launches += 2;
     ENG_TRY(cudaGetLastError());
     arenaTop = mark;  // the de-duplication set is no longer needed
@@ -1330,7 +1371,8 @@ int Engine::process_level_tt(const DeviceLevel &L, int remaining, unsigned long 
         }
     }
     arenaTop = mark;
-    k_tt_finish<<<nb, 256, 0, stream>>>(L.n, useTT && tt != nullptr, L.hash, L.acc, L.alias, L.root, parentAcc, tt,
+    k_tt_finish<<<nb, 256, 0, stream>>>(L.n, useTT && tt != nullptr, L.hash, L.hash2, L.acc, L.alias, L.root,
+                                        parentAcc, tt,
                                         ttMask, dTTStats);
     stats.other_launches++;
     if (rootOut) {

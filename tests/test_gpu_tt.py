@@ -79,3 +79,25 @@ def test_tt_with_chunked_levels(engine, golden):
         assert engine.stats()["chunked_levels"] > 0
     finally:
         engine.init(device=0, arena_bytes=8 << 30)
+
+
+def test_slot_key_collisions_stay_exact(engine, golden, oracle):
+    """Only 10 bits of the slot key kept: thousands of different positions
+    share each table slot and each de-duplication slot, so every hit and
+    every merge rests on the independent verification key."""
+    import os
+    os.environ["PERFT_TT_INDEX_KEY_BITS"] = "10"
+    try:
+        engine.init(device=0, arena_bytes=2 << 30, tt_log2_entries=16)
+        pos, depths, want = _golden(golden, max_leaves=5_000_000)
+        engine.reset_stats()
+        for _ in range(2):
+            assert np.array_equal(engine.perft_batch(pos, depths), want)
+        st = engine.stats()
+        assert st["tt_hits"] > 0 and st["tt_duplicates"] > 0
+        play = engine.random_playouts(seed=41, n=24, min_plies=4, max_plies=30)
+        got = engine.perft_batch(play, 4)
+        assert [int(x) for x in got] == [oracle.perft(p, 4) for p in play]
+    finally:
+        os.environ.pop("PERFT_TT_INDEX_KEY_BITS", None)
+        engine.init(device=0, arena_bytes=8 << 30)
