@@ -41,6 +41,7 @@ extern "C" {
 #define PERFT_ERR_TIMEOUT         -9
 #define PERFT_ERR_NOT_FOUND      -10
 #define PERFT_ERR_IO             -11
+#define PERFT_ERR_OVERFLOW       -12  /* a count does not fit 64 bits (the reference's InfInt range) */
 
 /* ---------------------------------------------------------------- types */
 
@@ -159,7 +160,11 @@ int perft_serve_get_stats(perft_serve_stats *out);
  * (a host transposition merge, like the reference's complete TT,
  * launcher.h:585-697) and searched on the GPU at the remaining depth.
  * moves/counts (optional, 256 entries) receive the per-move subtotals, the
- * divided perft of launcher.h:1344-1351. */
+ * divided perft of launcher.h:1344-1351.  Counts are 64-bit: when the total
+ * does not fit (the reference switches to InfInt there), PERFT_ERR_OVERFLOW
+ * is returned with every per-move subtotal filled in, to be summed wider by
+ * the caller; a subtotal that does not fit fails the call with the same
+ * status and *n_moves = 0. */
 int perft_deep(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, char (*moves)[6],
                uint64_t *counts, uint32_t *n_moves, uint64_t *total);
 /* One shard of perft_deep: only frontier boards i with i % n_shards == shard

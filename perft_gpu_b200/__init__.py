@@ -35,6 +35,7 @@ PERFT_ERR_ILLEGAL_MOVE = -8
 PERFT_ERR_TIMEOUT = -9
 PERFT_ERR_NOT_FOUND = -10
 PERFT_ERR_IO = -11
+PERFT_ERR_OVERFLOW = -12
 
 SLIDERS_AUTO = -1
 SLIDERS_KOGGE = 0
@@ -282,11 +283,13 @@ def deep(pos, depth: int, split_plies: int = 2, shard: int = 0, n_shards: int = 
     moves = (ctypes.c_char * (6 * 256))()
     counts = (ctypes.c_uint64 * 256)()
     n, total = ctypes.c_uint32(0), ctypes.c_uint64(0)
-    _check(lib().perft_deep_shard(ctypes.byref(p), int(depth), int(split_plies), int(shard), int(n_shards), moves,
-                                  counts, ctypes.byref(n), ctypes.byref(total)), "perft_deep_shard")
+    rc = lib().perft_deep_shard(ctypes.byref(p), int(depth), int(split_plies), int(shard), int(n_shards), moves,
+                                counts, ctypes.byref(n), ctypes.byref(total))
+    if rc != PERFT_ERR_OVERFLOW or n.value == 0:  # a total beyond 64 bits: the subtotals are exact, sum them here
+        _check(rc, "perft_deep_shard")
     raw = bytes(moves)
     div = {raw[6 * i:6 * i + 6].split(b"\0")[0].decode(): int(counts[i]) for i in range(n.value)}
-    return int(total.value), div
+    return sum(div.values()), div
 
 
 def store_open(path: Optional[str] = None) -> None:

@@ -73,27 +73,43 @@ void usage()
            "      perft_gpu --uci\n");
 }
 
-// Divided count of pos at depth: one subtotal per root move.
+typedef unsigned __int128 u128;
+
+// Decimal digits of a 128-bit count (totals beyond 64 bits: perft 14+).
+std::string to_dec(u128 v)
+{
+    std::string s;
+    do {
+        s.insert(s.begin(), (char)('0' + (int)(v % 10)));
+        v /= 10;
+    } while (v);
+    return s;
+}
+
+// Divided count of pos at depth: one subtotal per root move, summed in 128
+// bits (the engine reports PERFT_ERR_OVERFLOW when only the total exceeds 64
+// bits, with the subtotals filled in).
 int divided(const perft_pos48 &pos, uint32_t depth, std::vector<std::string> &moves,
-            std::vector<uint64_t> &counts, uint64_t *total)
+            std::vector<uint64_t> &counts, u128 *total)
 {
     char mv[256][6];
     uint64_t c[256];
     uint32_t n = 0;
+    uint64_t t64 = 0;
     int rc;
     if (depth > 10) {
-        rc = perft_deep(&pos, depth, depth - 7 < 4 ? depth - 7 : 4, mv, c, &n, total);
+        rc = perft_deep(&pos, depth, depth - 7 < 4 ? depth - 7 : 4, mv, c, &n, &t64);
     } else {
         rc = perft_divide(&pos, depth, mv, c, &n);
-        *total = 0;
-        for (uint32_t i = 0; rc == PERFT_OK && i < n; i++) *total += c[i];
     }
-    if (rc != PERFT_OK) return rc;
+    if (rc != PERFT_OK && !(rc == PERFT_ERR_OVERFLOW && n > 0)) return rc;
     moves.clear();
     counts.clear();
+    *total = 0;
     for (uint32_t i = 0; i < n; i++) {
         moves.emplace_back(mv[i]);
         counts.push_back(c[i]);
+        *total += c[i];
     }
     return PERFT_OK;
 }
@@ -120,7 +136,7 @@ int run_cli(int argc, char **argv)
     const int minDepth = maxDepth < 3 ? maxDepth : 3;
     for (int d = minDepth; d <= maxDepth; d++) {
         const double t0 = now_s();
-        uint64_t total = 0;
+        u128 total = 0;
         if (d > 10) {
             std::vector<std::string> mv;
             std::vector<uint64_t> c;
@@ -128,13 +144,15 @@ int run_cli(int argc, char **argv)
             if (rc == PERFT_OK)
                 for (size_t i = 0; i < mv.size(); i++) printf("%s   %20llu\n", mv[i].c_str(), (unsigned long long)c[i]);
         } else {
-            rc = perft(&pos, (uint32_t)d, &total);
+            uint64_t t64 = 0;
+            rc = perft(&pos, (uint32_t)d, &t64);
+            total = t64;
         }
         if (rc != PERFT_OK) {
             fprintf(stderr, "perft(%d) failed: %s\n", d, perft_status_string(rc));
             return 1;
         }
-        printf("Perft(%02d):%20llu, time: %8g s\n", d, (unsigned long long)total, now_s() - t0);
+        printf("Perft(%02d):%20s, time: %8g s\n", d, to_dec(total).c_str(), now_s() - t0);
         fflush(stdout);
     }
     return 0;
@@ -229,7 +247,7 @@ int run_uci()
             } else if (ensure_init() == PERFT_OK) {
                 std::vector<std::string> mv;
                 std::vector<uint64_t> c;
-                uint64_t total = 0;
+                u128 total = 0;
                 const double t0 = now_s();
                 const int rc = divided(pos, (uint32_t)depth, mv, c, &total);
                 if (rc != PERFT_OK) {
@@ -237,8 +255,8 @@ int run_uci()
                 } else {
                     for (size_t k = 0; k < mv.size(); k++) printf("%s: %llu\n", mv[k].c_str(), (unsigned long long)c[k]);
                     const double dt = now_s() - t0;
-                    printf("\nNodes searched: %llu\ninfo string time %g s, %g leaves/s\n\n", (unsigned long long)total,
-                           dt, dt > 0 ? (double)total / dt : 0.0);
+                    printf("\nNodes searched: %s\ninfo string time %g s, %g leaves/s\n\n", to_dec(total).c_str(), dt,
+                           dt > 0 ? (double)total / dt : 0.0);
                 }
             } else {
                 printf("info string no GPU engine\n");

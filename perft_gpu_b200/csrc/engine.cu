@@ -1757,6 +1757,7 @@ const char *perft_status_string(int status)
     case PERFT_ERR_TIMEOUT: return "timed out";
     case PERFT_ERR_NOT_FOUND: return "not found";
     case PERFT_ERR_IO: return "file I/O error";
+    case PERFT_ERR_OVERFLOW: return "count does not fit 64 bits";
     default: return "unknown status";
     }
 }

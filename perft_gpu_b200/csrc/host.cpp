@@ -452,17 +452,24 @@ int perft_deep_shard(const perft_pos48 *pos, uint32_t depth, uint32_t split_plie
     std::vector<u64> sub;
     const int rc = frontier_counts(f, depth - 1 - split_plies, shard, n_shards, sub);
     if (rc != PERFT_OK) return rc;
-    u64 sum = 0;
+    // 128-bit sums: a per-move subtotal must fit 64 bits; a total that does
+    // not (perft 14 of the initial position and beyond) is reported as
+    // PERFT_ERR_OVERFLOW with the subtotals filled in
+    unsigned __int128 sum = 0;
     for (size_t i = 0; i < mv.size(); i++) {
-        u64 s = 0;
-        for (const auto &kv : f.paths[i]) s += sub[kv.first] * kv.second;
+        unsigned __int128 s = 0;
+        for (const auto &kv : f.paths[i]) s += (unsigned __int128)sub[kv.first] * kv.second;
+        if (s >> 64) {
+            if (n_moves) *n_moves = 0;  // no usable subtotals
+            return PERFT_ERR_OVERFLOW;
+        }
         if (moves) move_to_uci(b, mv[i], moves[i]);
-        if (counts) counts[i] = s;
+        if (counts) counts[i] = (u64)s;
         sum += s;
     }
     if (n_moves) *n_moves = (uint32_t)mv.size();
-    *total = sum;
-    return PERFT_OK;
+    *total = (u64)sum;
+    return (sum >> 64) ? PERFT_ERR_OVERFLOW : PERFT_OK;
 }
 
 int perft_deep(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, char (*moves)[6],

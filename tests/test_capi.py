@@ -35,7 +35,7 @@ def test_probe_library_exports():
 
 
 def test_status_strings():
-    for code in range(0, -12, -1):
+    for code in range(0, -13, -1):
         assert pg._status_string(code) != "unknown status"
 
 
