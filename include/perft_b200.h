@@ -82,7 +82,9 @@ int perft_shutdown(void);
 const char *perft_status_string(int status);
 
 /* Leaf count of one position: perft_bb / perftLauncher
- * (perft_bb.h:79-101, launcher.h:1455-1503), returned instead of printed. */
+ * (perft_bb.h:79-101, launcher.h:1455-1503), returned instead of printed.
+ * The count must fit 64 bits (up to perft 13 of the initial position);
+ * perft_deep reports larger totals through exact per-move subtotals. */
 int perft(const perft_pos48 *pos, uint32_t depth, uint64_t *out);
 
 /* Batched perft: out[i] = perft(pos[i], depths[i]).  Host buffers.
