@@ -3,6 +3,8 @@
 // of the move generator for move lists only; every leaf count is computed by
 // the GPU engine (engine.cu).
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <mutex>
 #include <random>
 #include <string>
@@ -83,33 +85,71 @@ struct BoardKeyHash {
     }
 };
 
+constexpr int MAX_MOVES_BUF = 256;  // more than the 218 legal moves any position has
+
+struct ArraySink {
+    u32 *m;
+    u32 n;
+    void operator()(u32 x) { m[n++] = x; }
+};
+
+using BoardCounts = std::unordered_map<BoardKey, u64, BoardKeyHash>;
+
+BoardKey key_of(const Board &b) { return BoardKey{{b.mine, b.pawns & ~SIDE_BIT, b.knights, b.bq, b.rq, b.kings}}; }
+
+// Distinct boards `plies` below b with the number of paths reaching each.
+void enumerate_counts(const Board &b, u32 plies, BoardCounts &out)
+{
+    if (plies == 0) {
+        out[key_of(b)] += 1;
+        return;
+    }
+    u32 mv[MAX_MOVES_BUF];
+    ArraySink sink{mv, 0};
+    gen_moves<SV_KOGGE>(b, sink);
+    for (u32 i = 0; i < sink.n; i++) enumerate_counts(make_child(b, mv[i]), plies - 1, out);
+}
+
 struct Frontier {
     std::unordered_map<BoardKey, u32, BoardKeyHash> index;
     std::vector<BoardKey> boards;
     // (distinct board, path count) per root move
-    std::vector<std::unordered_map<u32, u64>> paths;
+    std::vector<std::vector<std::pair<u32, u64>>> paths;
 
-    void add(u32 root, const Board &b, u64 mult)
+    // Root moves are enumerated on all host cores, each into its own map;
+    // the maps are then merged in root-move order, so the board order (which
+    // the shards of a multi-process run rely on) does not depend on timing.
+    void build(const Board &root, const std::vector<u32> &mv, u32 plies)
     {
-        const BoardKey k{{b.mine, b.pawns & ~SIDE_BIT, b.knights, b.bq, b.rq, b.kings}};
-        auto it = index.find(k);
-        u32 id;
-        if (it == index.end()) {
-            id = (u32)boards.size();
-            index.emplace(k, id);
-            boards.push_back(k);
-        } else {
-            id = it->second;
+        const size_t R = mv.size();
+        std::vector<BoardCounts> local(R);
+        std::atomic<size_t> next{0};
+        auto work = [&]() {
+            for (size_t i; (i = next.fetch_add(1)) < R;) enumerate_counts(make_child(root, mv[i]), plies, local[i]);
+        };
+        unsigned T = std::max(1u, std::thread::hardware_concurrency());
+        if (T > R) T = (unsigned)std::max<size_t>(R, 1);
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < T; t++) pool.emplace_back(work);
+        work();
+        for (auto &t : pool) t.join();
+        paths.assign(R, {});
+        for (size_t i = 0; i < R; i++) {
+            paths[i].reserve(local[i].size());
+            for (const auto &kv : local[i]) {
+                auto it = index.find(kv.first);
+                u32 id;
+                if (it == index.end()) {
+                    id = (u32)boards.size();
+                    index.emplace(kv.first, id);
+                    boards.push_back(kv.first);
+                } else {
+                    id = it->second;
+                }
+                paths[i].emplace_back(id, kv.second);
+            }
+            BoardCounts().swap(local[i]);
         }
-        paths[root][id] += mult;
-    }
-    void enumerate(u32 root, const Board &b, u32 plies)
-    {
-        if (plies == 0) {
-            add(root, b, 1);
-            return;
-        }
-        for (u32 m : legal_moves(b)) enumerate(root, make_child(b, m), plies - 1);
     }
 };
 
@@ -447,8 +487,11 @@ int perft_deep_shard(const perft_pos48 *pos, uint32_t depth, uint32_t split_plie
     const Board b = from_pos48(pos->bb);
     const std::vector<u32> mv = legal_moves(b);
     Frontier f;
-    f.paths.resize(mv.size());
-    for (size_t i = 0; i < mv.size(); i++) f.enumerate((u32)i, make_child(b, mv[i]), split_plies);
+    try {
+        f.build(b, mv, split_plies);
+    } catch (const std::exception &) {
+        return PERFT_ERR_OUT_OF_MEMORY;  // host memory or threads exhausted
+    }
     std::vector<u64> sub;
     const int rc = frontier_counts(f, depth - 1 - split_plies, shard, n_shards, sub);
     if (rc != PERFT_OK) return rc;
