@@ -5,12 +5,16 @@
 //       every depth from 3 (or depth, if smaller) up to <depth>, each with
 //       its wall time.  Above depth 10 the root moves' subtotals are printed
 //       first, as the reference's divided perft does (launcher.h:1344-1351),
-//       computed by the host root split with transposition merging.  <gpus>
-//       is accepted for command-line compatibility; one process drives one
-//       GPU (CUDA_VISIBLE_DEVICES / PERFT_DEVICE pick it).  <launchdepth> is
-//       accepted and ignored: level sizes are planned from measured counts.
+//       computed by the host root split with transposition merging.  With
+//       <gpus> above 1 those deep counts are split over that many GPUs (the
+//       reference's one host thread per GPU, launcher.h:409-583): one shard
+//       process per GPU (GPU i runs perft_deep_shard shard i of <gpus>), and
+//       the per-move subtotals are summed here.  Shallower depths run on one
+//       GPU (PERFT_DEVICE).  <launchdepth> is accepted and ignored: level
+//       sizes are planned from measured counts.
 //       With PERFT_STORE=<file> the subtrees finished by a deep run are kept
 //       in that file, and a stopped run started again skips them.
+//       PERFT_DIVIDED_DEPTH moves the divided threshold (default 10).
 //   perft_gpu --records <file> [<depth>]
 //       Records mode (launcher.h:1579-1695): "<line> <perft> <perft*count>"
 //       per input line appended to <file>.op, resuming after the lines
@@ -21,7 +25,10 @@
 //       (UciInterface.cpp:7); "go perft" prints one "move: count" line per
 //       root move, then "Nodes searched: N".
 #include <chrono>
+#include <map>
 #include <stdio.h>
+#include <sys/wait.h>
+#include <unistd.h>
 #include <stdlib.h>
 #include <string.h>
 #include <string>
@@ -75,6 +82,24 @@ void usage()
 
 typedef unsigned __int128 u128;
 
+// Depths above this print divided output through the deep path (the
+// reference's DIVIDED_PERFT_DEPTH, launcher.h:21); PERFT_DIVIDED_DEPTH
+// overrides it.
+int divided_from()
+{
+    const char *e = getenv("PERFT_DIVIDED_DEPTH");
+    return e ? atoi(e) : 10;
+}
+
+// Host split of a deep count: the frontier sits 1 + split plies below the
+// root, at most five (about 10^6 distinct boards from the initial position).
+uint32_t split_for(uint32_t depth)
+{
+    uint32_t s = depth > 8 ? depth - 7 : 1;
+    if (s > 4) s = 4;
+    return s + 1 > depth ? depth - 1 : s;
+}
+
 // Decimal digits of a 128-bit count (totals beyond 64 bits: perft 14+).
 std::string to_dec(u128 v)
 {
@@ -84,6 +109,100 @@ std::string to_dec(u128 v)
         v /= 10;
     } while (v);
     return s;
+}
+
+// Deep divided count split over `gpus` shard processes: this program is
+// re-executed as "--deep-shard <i> <n> <depth> <split> <fen>" once per GPU
+// (a fresh process each, so every one initialises CUDA itself), each prints
+// "<move> <subtotal>" lines and "END", and the subtotals are summed here.
+int divided_sharded(const std::string &fen, uint32_t depth, uint32_t split, int gpus, std::vector<std::string> &moves,
+                    std::vector<uint64_t> &counts, u128 *total)
+{
+    std::vector<pid_t> pids;
+    std::vector<FILE *> outs;
+    const std::string dep = std::to_string(depth), spl = std::to_string(split), n = std::to_string(gpus);
+    for (int i = 0; i < gpus; i++) {
+        int fd[2];
+        if (pipe(fd) != 0) return PERFT_ERR_INTERNAL;
+        const pid_t pid = fork();
+        if (pid < 0) return PERFT_ERR_INTERNAL;
+        if (pid == 0) {
+            dup2(fd[1], 1);
+            close(fd[0]);
+            close(fd[1]);
+            const std::string si = std::to_string(i);
+            execl("/proc/self/exe", "perft_gpu", "--deep-shard", si.c_str(), n.c_str(), dep.c_str(), spl.c_str(),
+                  fen.c_str(), (char *)nullptr);
+            _exit(127);
+        }
+        close(fd[1]);
+        pids.push_back(pid);
+        outs.push_back(fdopen(fd[0], "r"));
+    }
+    std::map<std::string, uint64_t> sum;
+    std::vector<std::string> order;
+    bool ok = true;
+    for (size_t i = 0; i < outs.size(); i++) {
+        char line[256];
+        bool ended = false;
+        while (outs[i] && fgets(line, sizeof line, outs[i])) {
+            char mv[16];
+            unsigned long long c = 0;
+            if (!strncmp(line, "END", 3)) {
+                ended = true;
+                break;
+            }
+            if (sscanf(line, "%15s %llu", mv, &c) != 2) continue;
+            if (!sum.count(mv)) order.push_back(mv);
+            sum[mv] += c;
+        }
+        if (outs[i]) fclose(outs[i]);
+        ok = ok && ended;
+    }
+    for (pid_t pid : pids) {
+        int st = 0;
+        if (waitpid(pid, &st, 0) < 0 || !WIFEXITED(st) || WEXITSTATUS(st) != 0) ok = false;
+    }
+    if (!ok) return PERFT_ERR_INTERNAL;
+    moves.clear();
+    counts.clear();
+    *total = 0;
+    for (const std::string &m : order) {
+        moves.push_back(m);
+        counts.push_back(sum[m]);
+        *total += sum[m];
+    }
+    return PERFT_OK;
+}
+
+// One shard of a deep divided count (the child side of divided_sharded):
+// device = shard index unless PERFT_SHARD_DEVICE pins every shard to one GPU.
+int run_deep_shard(int argc, char **argv)
+{
+    if (argc < 7) return 2;
+    const uint32_t shard = (uint32_t)atoi(argv[2]), n = (uint32_t)atoi(argv[3]);
+    const uint32_t depth = (uint32_t)atoi(argv[4]), split = (uint32_t)atoi(argv[5]);
+    perft_pos48 pos;
+    if (perft_fen_to_pos(argv[6], &pos) != PERFT_OK) return 2;
+    if (!getenv("PERFT_SHARD_DEVICE")) {
+        char dev[16];
+        snprintf(dev, sizeof dev, "%u", shard);
+        setenv("PERFT_DEVICE", dev, 1);
+    } else {
+        setenv("PERFT_DEVICE", getenv("PERFT_SHARD_DEVICE"), 1);
+    }
+    if (ensure_init() != PERFT_OK) return 1;
+    char mv[256][6];
+    uint64_t c[256], t = 0;
+    uint32_t nm = 0;
+    const int rc = perft_deep_shard(&pos, depth, split, shard, n, mv, c, &nm, &t);
+    if (rc != PERFT_OK && !(rc == PERFT_ERR_OVERFLOW && nm > 0)) {
+        fprintf(stderr, "shard %u failed: %s\n", shard, perft_status_string(rc));
+        return 1;
+    }
+    for (uint32_t i = 0; i < nm; i++) printf("%s %llu\n", mv[i], (unsigned long long)c[i]);
+    printf("END\n");
+    return 0;
 }
 
 // Divided count of pos at depth: one subtotal per root move, summed in 128
@@ -97,8 +216,8 @@ int divided(const perft_pos48 &pos, uint32_t depth, std::vector<std::string> &mo
     uint32_t n = 0;
     uint64_t t64 = 0;
     int rc;
-    if (depth > 10) {
-        rc = perft_deep(&pos, depth, depth - 7 < 4 ? depth - 7 : 4, mv, c, &n, &t64);
+    if (depth > divided_from()) {
+        rc = perft_deep(&pos, depth, split_for(depth), mv, c, &n, &t64);
     } else {
         rc = perft_divide(&pos, depth, mv, c, &n);
     }
@@ -119,7 +238,8 @@ int run_cli(int argc, char **argv)
     std::string fen = argv[1];
     if (fen == "startpos" || fen.size() <= 5) fen = START_FEN;
     const int maxDepth = atoi(argv[2]);
-    if (maxDepth < 0 || maxDepth > 30) {
+    const int gpus = argc >= 4 ? atoi(argv[3]) : 1;
+    if (maxDepth < 0 || maxDepth > 30 || gpus < 1 || gpus > 64) {
         usage();
         return 2;
     }
@@ -129,7 +249,7 @@ int run_cli(int argc, char **argv)
         fprintf(stderr, "bad FEN: %s\n", perft_status_string(rc));
         return 2;
     }
-    if ((rc = ensure_init()) != PERFT_OK) return 1;
+    if (!(gpus > 1 && (maxDepth < 3 ? maxDepth : 3) > divided_from()) && (rc = ensure_init()) != PERFT_OK) return 1;
     char canon[128];
     perft_pos_to_fen(&pos, canon, sizeof canon);
     printf("%s\n", canon);
@@ -137,14 +257,20 @@ int run_cli(int argc, char **argv)
     for (int d = minDepth; d <= maxDepth; d++) {
         const double t0 = now_s();
         u128 total = 0;
-        if (d > 10) {
+        if (d > divided_from()) {
             std::vector<std::string> mv;
             std::vector<uint64_t> c;
-            rc = divided(pos, (uint32_t)d, mv, c, &total);
+            if (gpus > 1 && g_ready) {
+                perft_shutdown();  // the shard processes take the GPUs (and their memory) from here on
+                g_ready = false;
+            }
+            rc = gpus > 1 ? divided_sharded(fen, (uint32_t)d, split_for((uint32_t)d), gpus, mv, c, &total)
+                          : divided(pos, (uint32_t)d, mv, c, &total);
             if (rc == PERFT_OK)
                 for (size_t i = 0; i < mv.size(); i++) printf("%s   %20llu\n", mv[i].c_str(), (unsigned long long)c[i]);
         } else {
             uint64_t t64 = 0;
+            if (!g_ready && (rc = ensure_init()) != PERFT_OK) return 1;
             rc = perft(&pos, (uint32_t)d, &t64);
             total = t64;
         }
@@ -280,6 +406,11 @@ int main(int argc, char **argv)
     }
     if (argc >= 2 && !strcmp(argv[1], "--uci")) return run_uci();
     if (argc >= 2 && !strcmp(argv[1], "--records")) return run_records(argc, argv);
+    if (argc >= 2 && !strcmp(argv[1], "--deep-shard")) {
+        const int rc = run_deep_shard(argc, argv);
+        if (g_ready) perft_shutdown();
+        return rc;
+    }
     if (argc < 3) {
         usage();
         printf("\nAs no parameters were provided... running the start position to depth 5\n");

@@ -182,3 +182,22 @@ def test_store_resume_skips_finished_subtrees(stored, tmp_path, golden):
     assert again == want and div2 == div
     assert stored.stats()["leaf_launches"] == 0
     assert stored.store_stats()["appended"] == 0
+
+
+def test_cli_sharded_deep_counts(golden):
+    """perft_gpu <fen> <depth> <gpus>: the deep counts split over shard
+    processes (all pinned to this GPU here) and summed; divided output from
+    depth 7 on, every line equal to the single-process counts."""
+    env = dict(ENV, PERFT_DIVIDED_DEPTH="6", PERFT_SHARD_DEVICE="0", PERFT_ARENA_GB="3")
+    r = subprocess.run([CLI, "startpos", "7", "3"], capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr
+    counts = _by_name(golden, "initial_position")["counts"]
+    got, div = {}, {}
+    for line in r.stdout.splitlines():
+        if line.startswith("Perft("):
+            got[int(line[6:8])] = int(line.split(":")[1].split(",")[0])
+        elif len(line.split()) == 2:
+            m, c = line.split()
+            div[m] = int(c)
+    assert got == {d: counts[str(d)] for d in (3, 4, 5, 6, 7)}
+    assert len(div) == 20 and sum(div.values()) == counts["7"]
