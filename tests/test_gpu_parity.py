@@ -177,3 +177,16 @@ def test_many_move_positions(engine, oracle):
     engine.init(device=0, arena_bytes=8 << 30)
     d4 = engine.perft_batch(pos[:2], 4)
     assert [int(x) for x in d4] == [oracle.perft(p, 4) for p in pos[:2]]
+
+
+def test_colour_mirror_property(engine):
+    """Size-independent property at sizes the oracle cannot reach quickly:
+    a position and its colour mirror (ranks reversed, colours and side to
+    move swapped) have the same perft, here at depth 5 over 64 playouts."""
+    from tests._positions import mirror_fen
+    pos = engine.random_playouts(seed=51, n=64, min_plies=6, max_plies=40)
+    mir = np.stack([engine.fen_to_pos(mirror_fen(engine.pos_to_fen(p))) for p in pos])
+    a = engine.perft_batch(pos, 5)
+    b = engine.perft_batch(mir, 5)
+    assert np.array_equal(a, b)
+    assert int(a.sum()) > 10**9
