@@ -59,7 +59,10 @@ namespace {
 #ifndef PG_TILE_MINB
 #define PG_TILE_MINB 3
 #endif
-constexpr int TILE_NT = 256;
+#ifndef PG_TILE_NT
+#define PG_TILE_NT 256
+#endif
+constexpr int TILE_NT = PG_TILE_NT;  // threads per tile CTA
 constexpr int TILE_CAP_LOG2 = PG_TILE_CAP_LOG2;  // largest tile: 2^TILE_CAP_LOG2 items
 constexpr int TILE_CAP = 1 << TILE_CAP_LOG2;
 constexpr int TILE_MIN_LOG2 = 10;  // small levels use tiles down to 1024 items to fill every SM
