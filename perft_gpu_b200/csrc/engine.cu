@@ -858,6 +858,7 @@ public:
     void release_block() { arenaTop = blockMark; }
     u64 free_bytes() const { return arena_free(); }
     int device_id() const { return device; }
+    int leaf_sliders() const { return svLeaf; }
     u64 blockMark = 0;
     int tt_clear();
     void read_tt_stats()

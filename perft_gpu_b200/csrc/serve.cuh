@@ -126,6 +126,7 @@ private:
     u64 budget = 0, reserved = 0, stepItems = 0;
     u32 maxInFlight = 0, inFlight = 0, maxSlotUsed = 0;
     int gridLeaf = 0, gridExpand = 0;
+    bool leafSplit = false;
     int idleIterations = 0;
     // statistics
     u64 submitted = 0, completed = 0, iterations = 0, launches = 0, admittedBatches = 0;
@@ -203,11 +204,20 @@ int Server::start(const perft_serve_config &cfg, char *block, u64 bytes, int dev
     if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return PERFT_ERR_CUDA;
     cudaFuncSetAttribute(k_tile<MODE_LEAF, SV_KOGGE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)TILE_DYN_SMEM);
+    cudaFuncSetAttribute(k_tile<MODE_LEAF, SV_KOGGE_SPLIT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)TILE_DYN_SMEM);
     cudaFuncSetAttribute(k_tile<MODE_EXPAND, SV_KOGGE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)TILE_DYN_SMEM);
+    // the count-only ply follows the engine's tuned leaf variant when it is
+    // the split-shift Kogge-Stone one; every other choice uses plain Kogge-Stone
+    leafSplit = g_engine.leaf_sliders() == SV_KOGGE_SPLIT;
     int perSm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_tile<MODE_LEAF, SV_KOGGE, true>, TILE_NT,
-                                                  TILE_DYN_SMEM);
+    if (leafSplit)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_tile<MODE_LEAF, SV_KOGGE_SPLIT, true>, TILE_NT,
+                                                      TILE_DYN_SMEM);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_tile<MODE_LEAF, SV_KOGGE, true>, TILE_NT,
+                                                      TILE_DYN_SMEM);
     gridLeaf = std::max(1, perSm) * prop.multiProcessorCount;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_tile<MODE_EXPAND, SV_KOGGE, true>, TILE_NT,
                                                   TILE_DYN_SMEM);
@@ -449,7 +459,10 @@ int Server::launch(int mode, ServeLevel &S, u64 lo, u64 hi, DeviceLevel *child)
     P.err = dErr;
     const u64 nTiles = (hi - lo + TILE_CAP - 1) / TILE_CAP;
     if (cudaMemsetAsync(dCounter, 0, 4, st) != cudaSuccess) return PERFT_ERR_CUDA;
-    if (mode == MODE_LEAF)
+    if (mode == MODE_LEAF && leafSplit)
+        k_tile<MODE_LEAF, SV_KOGGE_SPLIT, true>
+            <<<(int)std::min<u64>(gridLeaf, nTiles), TILE_NT, TILE_DYN_SMEM, st>>>(P);
+    else if (mode == MODE_LEAF)
         k_tile<MODE_LEAF, SV_KOGGE, true><<<(int)std::min<u64>(gridLeaf, nTiles), TILE_NT, TILE_DYN_SMEM, st>>>(P);
     else
         k_tile<MODE_EXPAND, SV_KOGGE, true><<<(int)std::min<u64>(gridExpand, nTiles), TILE_NT, TILE_DYN_SMEM, st>>>(P);
