@@ -55,6 +55,11 @@
 #ifndef PG_GEN_MAGIC
 #define PG_GEN_MAGIC 1
 #endif
+// PG_GEN_MAGIC_ATTACKS 1: generation also builds the opponent's attack map
+// from magic lookups, one per opponent slider.
+#ifndef PG_GEN_MAGIC_ATTACKS
+#define PG_GEN_MAGIC_ATTACKS 1
+#endif
 
 #ifdef __CUDACC__
 #define PG_HD __host__ __device__ __forceinline__
@@ -925,7 +930,7 @@ PG_HD void gen_moves(const Board &b, Sink &out)
     // set-wise opponent attack map
     constexpr int GEN_SV = PG_GEN_MAGIC ? SV_MAGIC : SV;
     Ctx c;
-    setup_ctx<SV>(b, c);
+    setup_ctx<PG_GEN_MAGIC_ATTACKS ? GEN_SV : SV>(b, c);
     const u64 notMine = ~c.mine;
     emit_targets(out, c.ksq, PG_TAB(king[c.ksq]) & notMine & ~c.attacked);
     const u64 cm = check_mask<SV>(c);
