@@ -59,6 +59,9 @@ namespace {
 #ifndef PG_TILE_MINB
 #define PG_TILE_MINB 3
 #endif
+#ifndef PG_ONE_RUN_VOTE
+#define PG_ONE_RUN_VOTE 1  // one block vote for windows whose parents share one root
+#endif
 #ifndef PG_TILE_NT
 #define PG_TILE_NT 256
 #endif
@@ -487,14 +490,26 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
 
             int nRuns = 0;
             if (MODE == MODE_LEAF || TRACK) {
-                // parents are ordered by root: number the runs of equal roots
-                const bool head = valid && (tid == 0 || sroot[tid] != sroot[tid - 1]);
-                const int r = block_excl_count<TILE_NT>(head, swarp, nRuns);
-                if (valid) srun[tid] = head ? r : r - 1;
-                if (head) {
-                    srunRoot[r] = sroot[tid];
-                    sacc[r] = 0ull;
-                    if (TRACK) sdelta[r] = 0;
+                // parents are ordered by root: number the runs of equal roots.
+                // Usually the whole window belongs to one root, which one
+                // block vote settles without the two-barrier run count.
+                if (PG_ONE_RUN_VOTE && nP > 0 && __syncthreads_and(!valid || sroot[tid] == sroot[0])) {
+                    nRuns = 1;
+                    if (valid) srun[tid] = 0;
+                    if (tid == 0) {
+                        srunRoot[0] = sroot[0];
+                        sacc[0] = 0ull;
+                        if (TRACK) sdelta[0] = 0;
+                    }
+                } else {
+                    const bool head = valid && (tid == 0 || sroot[tid] != sroot[tid - 1]);
+                    const int r = block_excl_count<TILE_NT>(head, swarp, nRuns);
+                    if (valid) srun[tid] = head ? r : r - 1;
+                    if (head) {
+                        srunRoot[r] = sroot[tid];
+                        sacc[r] = 0ull;
+                        if (TRACK) sdelta[r] = 0;
+                    }
                 }
             }
 
