@@ -404,14 +404,18 @@ struct TileParams {
 
 // Emits a parent's moves, keeping only those whose global item index falls
 // inside [lo, hi): the window of the current tile.
+// Positions are relative to the window start: a parent starts at most
+// MAX_LEGAL_MOVES items before it and a window holds at most TILE_CAP items,
+// so 32 bits hold them and one unsigned compare does the bounds test.
 struct WindowSink {
     u32 *items;
-    u64 g, lo, hi;
+    int rel;  // next move's position relative to the window start
+    u32 n;    // window length
     u32 tag;
     __device__ __forceinline__ void operator()(u32 m)
     {
-        if (g >= lo && g < hi) items[g - lo] = tag | m;
-        ++g;
+        if ((u32)rel < n) items[rel] = tag | m;
+        ++rel;
     }
 };
 
@@ -517,9 +521,9 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
             // parents without items (none legal, or answered by the table) generate nothing
             if (valid && qEnd > qBeg && qEnd > sBeg && qBeg < sEnd) {
                 const Board b{sb[0][tid], sb[1][tid], sb[2][tid], sb[3][tid], sb[4][tid], sb[5][tid]};
-                WindowSink sink{sitems, qBeg, sBeg, sEnd, (u32)tid << 16};
+                WindowSink sink{sitems, (int)((long long)qBeg - (long long)sBeg), (u32)(sEnd - sBeg), (u32)tid << 16};
                 gen_moves<SV>(b, sink);
-                if (sink.g != qEnd) atomicOr(P.err, DERR_GEN_MISMATCH);
+                if ((long long)sink.rel != (long long)qEnd - (long long)sBeg) atomicOr(P.err, DERR_GEN_MISMATCH);
             }
             __syncthreads();
 
