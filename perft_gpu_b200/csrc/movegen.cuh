@@ -896,14 +896,28 @@ PG_HD u32 encode_move(int from, int to, u32 flags)
     return (flags << 12) | ((u32)to << 6) | (u32)from;
 }
 
+// Calls f(square) for every set bit in ascending order; on the device the
+// two 32-bit halves are walked separately (32-bit bit scans and clears).
+template <class F>
+PG_HD void for_each_bit(u64 x, F f)
+{
+#ifdef __CUDA_ARCH__
+    for (u32 w = (u32)x; w; w &= w - 1) f(__ffs(w) - 1);
+    for (u32 w = (u32)(x >> 32); w; w &= w - 1) f(__ffs(w) + 31);
+#else
+    while (x) {
+        f(ctz(x));
+        x &= x - 1;
+    }
+#endif
+}
+
 // Emits every target square of a piece as a move.
 template <class Sink>
 PG_HD void emit_targets(Sink &out, int from, u64 targets)
 {
-    while (targets) {
-        out(encode_move(from, ctz(targets), MF_QUIET));
-        targets &= targets - 1;
-    }
+    const u32 base = encode_move(from, 0, MF_QUIET);
+    for_each_bit(targets, [&](int to) { out(base | ((u32)to << 6)); });
 }
 
 // Pawn move to dst with the four promotions on the last rank.
@@ -992,29 +1006,11 @@ PG_HD void gen_moves(const Board &b, Sink &out)
     const u64 p1 = sh_n(P) & c.empty;
     u64 p1c = p1 & cm;
     u64 p2 = sh_n(p1 & RANK3) & c.empty & cm;
-    while (p1c) {
-        const int to = ctz(p1c);
-        p1c &= p1c - 1;
-        emit_pawn(out, to - 8, to, MF_QUIET);
-    }
-    while (p2) {
-        const int to = ctz(p2);
-        p2 &= p2 - 1;
-        out(encode_move(to - 16, to, MF_DOUBLE_PUSH));
-    }
+    for_each_bit(p1c, [&](int to) { emit_pawn(out, to - 8, to, MF_QUIET); });
+    for_each_bit(p2, [&](int to) { out(encode_move(to - 16, to, MF_DOUBLE_PUSH)); });
     const u64 capT = c.theirs & cm;
-    u64 cl = sh_nw(P) & capT;
-    while (cl) {
-        const int to = ctz(cl);
-        cl &= cl - 1;
-        emit_pawn(out, to - 7, to, MF_CAPTURE);
-    }
-    u64 cr = sh_ne(P) & capT;
-    while (cr) {
-        const int to = ctz(cr);
-        cr &= cr - 1;
-        emit_pawn(out, to - 9, to, MF_CAPTURE);
-    }
+    for_each_bit(sh_nw(P) & capT, [&](int to) { emit_pawn(out, to - 7, to, MF_CAPTURE); });
+    for_each_bit(sh_ne(P) & capT, [&](int to) { emit_pawn(out, to - 9, to, MF_CAPTURE); });
     const u32 epf = c.st >> 4;
     if (epf) {
         const u64 target = 1ULL << (39 + epf);
