@@ -641,19 +641,17 @@ PG_HD u32 count_moves_fused(const Board &b)
     // pin line
     u64 pinned = 0, slChk = 0;
     u32 nPinned = 0;
-    u64 snipers = (PG_TAB(rookRays[ksq]) & tR) | (PG_TAB(bishopRays[ksq]) & tB);
-    while (snipers) {
-        const int s = ctz(snipers);
-        snipers &= snipers - 1;
+    const u64 bRays = PG_TAB(bishopRays[ksq]);
+    for_each_bit((PG_TAB(rookRays[ksq]) & tR) | (bRays & tB), [&](int s) {
         const u64 btw = PG_TAB(between[ksq][s]);
         const u64 blk = btw & occ;
         if (!blk) {
             slChk |= 1ULL << s;
-            continue;
+            return;
         }
-        if ((blk & (blk - 1)) || !(blk & mine)) continue;
+        if ((blk & (blk - 1)) || !(blk & mine)) return;
         pinned |= blk;
-        const bool diag = (PG_TAB(bishopRays[ksq]) >> s) & 1;
+        const bool diag = (bRays >> s) & 1;
         if (blk & (diag ? b.bq : b.rq)) {
             nPinned += popc(btw);
         } else if (blk & pawns) {
@@ -665,7 +663,7 @@ PG_HD u32 count_moves_fused(const Board &b)
                 nPinned += popc(p1) + popc(sh_n(p1 & RANK3) & empty);
             }
         }
-    }
+    });
     const u64 chk = (pawn_att_up(myK) & tP) | (PG_TAB(knight[ksq]) & tN) | slChk;
     u64 cm = ~0ULL, xray = 0;
     if (chk) {
@@ -769,12 +767,9 @@ PG_HD u32 count_moves_fused(const Board &b)
     }
 
     // knights
-    u64 N = b.knights & mine & ~pinned;
+    const u64 N = b.knights & mine & ~pinned;
     if (PG_KNIGHT_LUT) {
-        while (N) {
-            n += popc(PG_TAB(knight[ctz(N)]) & targets);
-            N &= N - 1;
-        }
+        for_each_bit(N, [&](int sq) { n += popc(PG_TAB(knight[sq]) & targets); });
     } else {
         n += knight_set_count(N, targets);
     }
@@ -984,24 +979,10 @@ PG_HD void gen_moves(const Board &b, Sink &out)
     }
 
     // free pieces
-    u64 N = b.knights & c.mine & ~pinned;
-    while (N) {
-        const int s = ctz(N);
-        N &= N - 1;
-        emit_targets(out, s, PG_TAB(knight[s]) & targets);
-    }
-    u64 B = b.bq & c.mine & ~pinned;
-    while (B) {
-        const int s = ctz(B);
-        B &= B - 1;
-        emit_targets(out, s, bishop_att<GEN_SV>(s, c.occ) & targets);
-    }
-    u64 R = b.rq & c.mine & ~pinned;
-    while (R) {
-        const int s = ctz(R);
-        R &= R - 1;
-        emit_targets(out, s, rook_att<GEN_SV>(s, c.occ) & targets);
-    }
+    for_each_bit(b.knights & c.mine & ~pinned, [&](int s) { emit_targets(out, s, PG_TAB(knight[s]) & targets); });
+    for_each_bit(b.bq & c.mine & ~pinned,
+                 [&](int s) { emit_targets(out, s, bishop_att<GEN_SV>(s, c.occ) & targets); });
+    for_each_bit(b.rq & c.mine & ~pinned, [&](int s) { emit_targets(out, s, rook_att<GEN_SV>(s, c.occ) & targets); });
     const u64 P = c.pawns & c.mine & ~pinned;
     const u64 p1 = sh_n(P) & c.empty;
     u64 p1c = p1 & cm;
