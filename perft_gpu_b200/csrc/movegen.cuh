@@ -50,6 +50,10 @@
 #ifndef PG_KS_LINE
 #define PG_KS_LINE 1
 #endif
+// PG_CTZ32 1: bit scans of 64-bit words as two 32-bit scans.
+#ifndef PG_CTZ32
+#define PG_CTZ32 1
+#endif
 // PG_GEN_MAGIC 1: move generation looks up each slider's targets in the
 // magic tables whatever the slider variant.
 #ifndef PG_GEN_MAGIC
@@ -192,7 +196,13 @@ PG_HD int popc_lo(u64 x)
 PG_HD int ctz(u64 x)
 {
 #ifdef __CUDA_ARCH__
+#if PG_CTZ32
+    // two 32-bit scans and a select
+    const u32 lo = (u32)x;
+    return lo ? __ffs(lo) - 1 : __ffs((u32)(x >> 32)) + 31;
+#else
     return __ffsll((long long)x) - 1;
+#endif
 #else
     return __builtin_ctzll(x);
 #endif
