@@ -208,6 +208,22 @@ PG_HD int ctz(u64 x)
 #endif
 }
 
+// Calls f(square) for every set bit in ascending order; on the device the
+// two 32-bit halves are walked separately (32-bit bit scans and clears).
+template <class F>
+PG_HD void for_each_bit(u64 x, F f)
+{
+#ifdef __CUDA_ARCH__
+    for (u32 w = (u32)x; w; w &= w - 1) f(__ffs(w) - 1);
+    for (u32 w = (u32)(x >> 32); w; w &= w - 1) f(__ffs(w) + 31);
+#else
+    while (x) {
+        f(ctz(x));
+        x &= x - 1;
+    }
+#endif
+}
+
 // Vertical mirror (rank r -> 7 - r): a byte swap.
 PG_HD u64 flipv(u64 x)
 {
@@ -400,10 +416,7 @@ PG_HD u64 bishop_set_att(u64 set, u64 occ)
 {
     if (SvTraits<SV>::kogge) return ks_diag<SvTraits<SV>::shift>(set, ~occ);
     u64 a = 0;
-    while (set) {
-        a |= magic_bishop(ctz(set), occ);
-        set &= set - 1;
-    }
+    for_each_bit(set, [&](int sq) { a |= magic_bishop(sq, occ); });
     return a;
 }
 template <int SV>
@@ -411,10 +424,7 @@ PG_HD u64 rook_set_att(u64 set, u64 occ)
 {
     if (SvTraits<SV>::kogge) return ks_orth<SvTraits<SV>::shift>(set, ~occ);
     u64 a = 0;
-    while (set) {
-        a |= magic_rook(ctz(set), occ);
-        set &= set - 1;
-    }
+    for_each_bit(set, [&](int sq) { a |= magic_rook(sq, occ); });
     return a;
 }
 
@@ -476,14 +486,11 @@ PG_HD void setup_ctx(const Board &b, Ctx &c)
 // Pinned pieces of the side to move (findPinnedPieces, MoveGeneratorBitboard.h:1213-1249).
 PG_HD u64 pinned_of(const Ctx &c)
 {
-    u64 snipers = (PG_TAB(rookRays[c.ksq]) & c.tR) | (PG_TAB(bishopRays[c.ksq]) & c.tB);
     u64 pinned = 0;
-    while (snipers) {
-        int s = ctz(snipers);
-        snipers &= snipers - 1;
-        u64 blk = PG_TAB(between[c.ksq][s]) & c.occ;
+    for_each_bit((PG_TAB(rookRays[c.ksq]) & c.tR) | (PG_TAB(bishopRays[c.ksq]) & c.tB), [&](int s) {
+        const u64 blk = PG_TAB(between[c.ksq][s]) & c.occ;
         if (blk && !(blk & (blk - 1))) pinned |= blk & c.mine;
-    }
+    });
     return pinned;
 }
 
@@ -901,22 +908,6 @@ PG_HD u32 encode_move(int from, int to, u32 flags)
     return (flags << 12) | ((u32)to << 6) | (u32)from;
 }
 
-// Calls f(square) for every set bit in ascending order; on the device the
-// two 32-bit halves are walked separately (32-bit bit scans and clears).
-template <class F>
-PG_HD void for_each_bit(u64 x, F f)
-{
-#ifdef __CUDA_ARCH__
-    for (u32 w = (u32)x; w; w &= w - 1) f(__ffs(w) - 1);
-    for (u32 w = (u32)(x >> 32); w; w &= w - 1) f(__ffs(w) + 31);
-#else
-    while (x) {
-        f(ctz(x));
-        x &= x - 1;
-    }
-#endif
-}
-
 // Emits every target square of a piece as a move.
 template <class Sink>
 PG_HD void emit_targets(Sink &out, int from, u64 targets)
@@ -965,13 +956,10 @@ PG_HD void gen_moves(const Board &b, Sink &out)
     const u64 pinned = pinned_of(c);
 
     // pinned pieces: along the pin line only, never in check
-    u64 pp = inCheck ? 0 : pinned;
-    while (pp) {
-        const int s = ctz(pp);
-        const u64 p = pp & (0 - pp);
-        pp ^= p;
+    for_each_bit(inCheck ? 0 : pinned, [&](int s) {
+        const u64 p = 1ULL << s;
         const u64 line = PG_TAB(line[s][c.ksq]);
-        if (p & b.knights) continue;
+        if (p & b.knights) return;
         if (p & c.pawns) {
             const u64 p1 = sh_n(p) & c.empty & line;
             if (p1) {
@@ -980,13 +968,13 @@ PG_HD void gen_moves(const Board &b, Sink &out)
             }
             const u64 cap = pawn_att_up(p) & line & c.theirs;
             if (cap) emit_pawn(out, s, ctz(cap), MF_CAPTURE);
-            continue;
+            return;
         }
         u64 t = 0;
         if (p & b.bq) t |= bishop_att<GEN_SV>(s, c.occ);
         if (p & b.rq) t |= rook_att<GEN_SV>(s, c.occ);
         emit_targets(out, s, t & notMine & line);
-    }
+    });
 
     // free pieces
     for_each_bit(b.knights & c.mine & ~pinned, [&](int s) { emit_targets(out, s, PG_TAB(knight[s]) & targets); });
