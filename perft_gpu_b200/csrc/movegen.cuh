@@ -668,7 +668,7 @@ PG_HD u32 count_moves_fused(const Board &b)
         }
         if ((blk & (blk - 1)) || !(blk & mine)) return;
         pinned |= blk;
-        const bool diag = (bRays >> s) & 1;
+        const bool diag = ((ksq ^ s) & 7) != 0 && ((ksq ^ s) >> 3) != 0;  // neither same file nor same rank
         if (blk & (diag ? b.bq : b.rq)) {
             nPinned += popc(btw);
         } else if (blk & pawns) {
