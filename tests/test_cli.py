@@ -53,3 +53,13 @@ def test_fails_cleanly_without_gpu(cli, tmp_path):
     assert r.returncode == 0 and "info string no GPU engine" in r.stdout
     bad = subprocess.run([cli, "nonsense/fen w - -", "3"], capture_output=True, text=True, timeout=60)
     assert bad.returncode == 2 and "bad FEN" in bad.stderr
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="a GPU is present; covered by the gpu tests")
+def test_sharded_deep_fails_cleanly_without_gpu(cli):
+    """With <gpus> above 1 the deep depths run in shard processes; when they
+    cannot start an engine the parent reports the failure instead of a count."""
+    env = dict(os.environ, PERFT_DIVIDED_DEPTH="2")
+    r = subprocess.run([cli, "startpos", "3", "2"], capture_output=True, text=True, timeout=120, env=env)
+    assert r.returncode == 1
+    assert "perft(3) failed" in r.stderr and "Perft(03)" not in r.stdout
