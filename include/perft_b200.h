@@ -178,6 +178,12 @@ int perft_deep_shard(const perft_pos48 *pos, uint32_t depth, uint32_t split_plie
                      uint32_t n_shards, char (*moves)[6], uint64_t *counts, uint32_t *n_moves,
                      uint64_t *total);
 
+/* Size of the frontier perft_deep(pos, depth, split_plies) would search:
+ * distinct boards and the move paths reaching them (host only, no GPU), for
+ * choosing split_plies.  No counterpart in the reference. */
+int perft_deep_frontier(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, uint64_t *n_boards,
+                        uint64_t *n_paths);
+
 /* Result store for deep runs: the counts of completed frontier subtrees,
  * keyed by the exact board and remaining depth.  perft_deep / perft_deep_shard
  * look every frontier board up before searching it and add what they search.

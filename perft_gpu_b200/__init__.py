@@ -154,6 +154,7 @@ def _load():
         "perft_result_store_open": (ctypes.c_int, [ctypes.c_char_p]),
         "perft_result_store_close": (ctypes.c_int, []),
         "perft_result_store_stats": (ctypes.c_int, [u64p, u64p, u64p]),
+        "perft_deep_frontier": (ctypes.c_int, [P(_Pos48), ctypes.c_uint32, ctypes.c_uint32, u64p, u64p]),
         "perft_records": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, u64p]),
     }
     for name, (res, args) in sig.items():
@@ -290,6 +291,15 @@ def deep(pos, depth: int, split_plies: int = 2, shard: int = 0, n_shards: int = 
     raw = bytes(moves)
     div = {raw[6 * i:6 * i + 6].split(b"\0")[0].decode(): int(counts[i]) for i in range(n.value)}
     return sum(div.values()), div
+
+
+def deep_frontier(pos, depth: int, split_plies: int = 2):
+    """(distinct boards, move paths) of the frontier deep() would search; host only."""
+    p = _pos(pos)
+    nb, npaths = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    _check(lib().perft_deep_frontier(ctypes.byref(p), int(depth), int(split_plies), ctypes.byref(nb),
+                                     ctypes.byref(npaths)), "perft_deep_frontier")
+    return int(nb.value), int(npaths.value)
 
 
 def store_open(path: Optional[str] = None) -> None:

@@ -521,6 +521,32 @@ int perft_deep(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, cha
     return perft_deep_shard(pos, depth, split_plies, 0, 1, moves, counts, n_moves, total);
 }
 
+// Size of the frontier perft_deep(pos, depth, split_plies) would search: the
+// distinct boards 1 + split_plies plies below pos and the move paths that
+// reach them.  Host only: for planning a deep run's memory and time.
+int perft_deep_frontier(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, uint64_t *n_boards,
+                        uint64_t *n_paths)
+{
+    if (!pos || depth < 1 || depth > 30) return PERFT_ERR_INVALID_ARG;
+    if (!board_ok(pos)) return PERFT_ERR_INVALID_ARG;
+    if (split_plies + 1 > depth) split_plies = depth - 1;
+    build_tables();
+    const Board b = from_pos48(pos->bb);
+    const std::vector<u32> mv = legal_moves(b);
+    Frontier f;
+    try {
+        f.build(b, mv, split_plies);
+    } catch (const std::exception &) {
+        return PERFT_ERR_OUT_OF_MEMORY;
+    }
+    u64 paths = 0;
+    for (const auto &root : f.paths)
+        for (const auto &kv : root) paths += kv.second;
+    if (n_boards) *n_boards = f.boards.size();
+    if (n_paths) *n_paths = paths;
+    return PERFT_OK;
+}
+
 int perft_result_store_open(const char *path)
 {
     std::lock_guard<std::mutex> lk(g_store.mu);

@@ -3,6 +3,8 @@ check word, torn-tail recovery, and rejection of a foreign file.  Counts added
 by deep runs are covered by the gpu tests."""
 import struct
 
+import numpy as np
+
 import pytest
 
 import perft_gpu_b200 as pg
@@ -68,3 +70,21 @@ def test_memory_store_and_closed_stats(store):
     store.store_close()
     with pytest.raises(pg.PerftError):
         store.store_stats()
+
+
+def test_deep_frontier_merges_transpositions(oracle):
+    """The frontier deep perft searches: every move path to 1 + split plies,
+    merged into distinct boards.  Paths equal perft at that depth; boards
+    equal the distinct positions the oracle reaches (no GPU needed)."""
+    start = pg.fen_to_pos(pg.START_FEN)
+    mid = pg.random_playouts(seed=77, n=1, min_plies=10, max_plies=10)[0]
+    for pos, split in ((start, 1), (start, 2), (mid, 1)):
+        boards, paths = pg.deep_frontier(pos, 6, split)
+        level = [np.asarray(pos, dtype=np.uint64)]
+        for _ in range(split + 1):
+            level = [c for p in level for c in oracle.children(p)]
+        assert paths == len(level) == oracle.perft(pos, split + 1)
+        assert boards == len({tuple(int(x) for x in c) for c in level})
+        assert boards <= paths
+    boards, paths = pg.deep_frontier(start, 6, 2)
+    assert boards < paths  # ply 3 of the initial position already has transpositions
