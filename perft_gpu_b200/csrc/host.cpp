@@ -124,15 +124,28 @@ struct Frontier {
         const size_t R = mv.size();
         std::vector<BoardCounts> local(R);
         std::atomic<size_t> next{0};
+        std::atomic<bool> failed{false};
+        // an exception must not leave a worker thread (that would terminate
+        // the process): workers record it and the caller rethrows
         auto work = [&]() {
-            for (size_t i; (i = next.fetch_add(1)) < R;) enumerate_counts(make_child(root, mv[i]), plies, local[i]);
+            try {
+                for (size_t i; !failed && (i = next.fetch_add(1)) < R;)
+                    enumerate_counts(make_child(root, mv[i]), plies, local[i]);
+            } catch (...) {
+                failed = true;
+            }
         };
         unsigned T = std::max(1u, std::thread::hardware_concurrency());
         if (T > R) T = (unsigned)std::max<size_t>(R, 1);
         std::vector<std::thread> pool;
-        for (unsigned t = 1; t < T; t++) pool.emplace_back(work);
+        try {
+            for (unsigned t = 1; t < T; t++) pool.emplace_back(work);
+        } catch (...) {
+            // fewer threads than asked for: the started ones and this one finish the work
+        }
         work();
         for (auto &t : pool) t.join();
+        if (failed) throw std::bad_alloc();
         paths.assign(R, {});
         for (size_t i = 0; i < R; i++) {
             paths[i].reserve(local[i].size());
