@@ -279,6 +279,20 @@ int frontier_counts(const Frontier &f, u32 depth, u32 shard, u32 n_shards, std::
     return PERFT_OK;
 }
 
+// C-ABI functions return status codes: an exception (host memory
+// exhausted) must not cross the boundary.
+template <class F>
+int guarded(F f)
+{
+    try {
+        return f();
+    } catch (const std::bad_alloc &) {
+        return PERFT_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        return PERFT_ERR_INTERNAL;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -432,7 +446,7 @@ int perft_apply_uci_move(perft_pos48 *pos, const char *uci)
     return PERFT_ERR_ILLEGAL_MOVE;
 }
 
-int perft_divide(const perft_pos48 *pos, uint32_t depth, char (*moves)[6], uint64_t *counts,
+static int divide_impl(const perft_pos48 *pos, uint32_t depth, char (*moves)[6], uint64_t *counts,
                  uint32_t *n_moves)
 {
     if (!pos || !moves || !counts || !n_moves || depth < 1 || depth > 21) return PERFT_ERR_INVALID_ARG;
@@ -488,7 +502,7 @@ int perft_random_playouts(uint64_t seed, uint32_t n, uint32_t min_plies, uint32_
 // n_shards > 1 only every n_shards-th frontier board (from `shard`) is
 // searched, so the per-move subtotals of shards 0..n_shards-1 sum to the full
 // result: the multi-GPU root split, one process per GPU (launcher.h:476-583).
-int perft_deep_shard(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, uint32_t shard,
+static int deep_shard_impl(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, uint32_t shard,
                      uint32_t n_shards, char (*moves)[6], uint64_t *counts, uint32_t *n_moves, uint64_t *total)
 {
     if (!pos || !total || depth < 1 || depth > 30) return PERFT_ERR_INVALID_ARG;
@@ -537,7 +551,7 @@ int perft_deep(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, cha
 // Size of the frontier perft_deep(pos, depth, split_plies) would search: the
 // distinct boards 1 + split_plies plies below pos and the move paths that
 // reach them.  Host only: for planning a deep run's memory and time.
-int perft_deep_frontier(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, uint64_t *n_boards,
+static int deep_frontier_impl(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, uint64_t *n_boards,
                         uint64_t *n_paths)
 {
     if (!pos || depth < 1 || depth > 30) return PERFT_ERR_INVALID_ARG;
@@ -560,7 +574,7 @@ int perft_deep_frontier(const perft_pos48 *pos, uint32_t depth, uint32_t split_p
     return PERFT_OK;
 }
 
-int perft_result_store_open(const char *path)
+static int store_open_impl(const char *path)
 {
     std::lock_guard<std::mutex> lk(g_store.mu);
     if (g_store.f) fclose(g_store.f);
@@ -633,7 +647,7 @@ int perft_result_store_stats(uint64_t *entries, uint64_t *hits, uint64_t *append
 // appended to "<in_path>.op".  Lines already present in the output are
 // skipped, so an interrupted run resumes where it stopped.  Lines are
 // searched in GPU batches of `batch` records.
-int perft_records(const char *in_path, uint32_t depth, uint32_t batch, uint64_t *records_done)
+static int records_impl(const char *in_path, uint32_t depth, uint32_t batch, uint64_t *records_done)
 {
     if (!in_path || depth > 20) return PERFT_ERR_INVALID_ARG;
     if (!batch) batch = 4096;
@@ -720,6 +734,34 @@ int perft_position_features(const perft_pos48 *pos, uint32_t *features)
     if (c.attacked & c.myK) f |= 8;
     *features = f;
     return PERFT_OK;
+}
+
+int perft_divide(const perft_pos48 *pos, uint32_t depth, char (*moves)[6], uint64_t *counts, uint32_t *n_moves)
+{
+    return guarded([&] { return divide_impl(pos, depth, moves, counts, n_moves); });
+}
+
+int perft_deep_shard(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, uint32_t shard,
+                     uint32_t n_shards, char (*moves)[6], uint64_t *counts, uint32_t *n_moves, uint64_t *total)
+{
+    return guarded(
+        [&] { return deep_shard_impl(pos, depth, split_plies, shard, n_shards, moves, counts, n_moves, total); });
+}
+
+int perft_deep_frontier(const perft_pos48 *pos, uint32_t depth, uint32_t split_plies, uint64_t *n_boards,
+                        uint64_t *n_paths)
+{
+    return guarded([&] { return deep_frontier_impl(pos, depth, split_plies, n_boards, n_paths); });
+}
+
+int perft_result_store_open(const char *path)
+{
+    return guarded([&] { return store_open_impl(path); });
+}
+
+int perft_records(const char *in_path, uint32_t depth, uint32_t batch, uint64_t *records_done)
+{
+    return guarded([&] { return records_impl(in_path, depth, batch, records_done); });
 }
 
 }  // extern "C"
