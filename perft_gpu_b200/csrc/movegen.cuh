@@ -32,8 +32,8 @@
 
 #include <stdint.h>
 
-// Knight moves of the Kogge-Stone variants: 0 = eight jump shifts over the
-// whole knight set, 1 = one table lookup per knight.
+// Build-time alternatives, each kept for A/B measurement; the defaults are
+// the measured-fastest choices on B200.
 // PG_FUSED_COUNT 1: Kogge-Stone counts use count_moves_fused.
 #ifndef PG_FUSED_COUNT
 #define PG_FUSED_COUNT 1
@@ -42,6 +42,8 @@
 #ifndef PG_RANK_SUB
 #define PG_RANK_SUB 1
 #endif
+// PG_KNIGHT_LUT: knight moves of the Kogge-Stone variants; 0 = eight jump
+// shifts over the whole knight set, 1 = one table lookup per knight.
 #ifndef PG_KNIGHT_LUT
 #define PG_KNIGHT_LUT 1
 #endif
