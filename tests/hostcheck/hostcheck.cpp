@@ -33,6 +33,19 @@ uint64_t perft_rel(const Board &b, uint32_t depth)
 }
 }  // namespace
 
+// Calls f.template operator()<SV>() for the runtime variant sv (0..4).
+template <class F>
+auto with_sv(int sv, F f)
+{
+    switch (sv) {
+    case SV_MAGIC: return f.template operator()<SV_MAGIC>();
+    case SV_KOGGE_FMA: return f.template operator()<SV_KOGGE_FMA>();
+    case SV_KOGGE_SPLIT: return f.template operator()<SV_KOGGE_SPLIT>();
+    case SV_HYBRID: return f.template operator()<SV_HYBRID>();
+    default: return f.template operator()<SV_KOGGE>();
+    }
+}
+
 extern "C" {
 
 int hc_init(void)
@@ -43,19 +56,17 @@ int hc_init(void)
 
 uint32_t hc_count(const uint64_t pos[6], int sv)
 {
-    Board b = from_pos48(pos);
-    if (sv == 4) return count_moves<SV_HYBRID>(b);
-    return sv ? count_moves<SV_MAGIC>(b) : count_moves<SV_KOGGE>(b);
+    const Board b = from_pos48(pos);
+    return with_sv(sv, [&]<int SV>() { return count_moves<SV>(b); });
 }
 
 // Children of pos as pos48 boards; returns the number of moves.
 uint32_t hc_children(const uint64_t pos[6], int sv, uint64_t *out)
 {
-    Board b = from_pos48(pos);
+    const Board b = from_pos48(pos);
     u32 moves[256];
     VecSink s{moves, 0};
-    if (sv) gen_moves<SV_MAGIC>(b, s);
-    else gen_moves<SV_KOGGE>(b, s);
+    with_sv(sv, [&]<int SV>() { gen_moves<SV>(b, s); return 0; });
     for (u32 i = 0; i < s.n; i++) {
         Board c = make_child(b, moves[i]);
         to_pos48(c, out + 6 * i);
@@ -65,9 +76,8 @@ uint32_t hc_children(const uint64_t pos[6], int sv, uint64_t *out)
 
 uint64_t hc_perft(const uint64_t pos[6], uint32_t depth, int sv)
 {
-    Board b = from_pos48(pos);
-    if (sv == 4) return perft_rel<SV_HYBRID>(b, depth);
-    return sv ? perft_rel<SV_MAGIC>(b, depth) : perft_rel<SV_KOGGE>(b, depth);
+    const Board b = from_pos48(pos);
+    return with_sv(sv, [&]<int SV>() { return perft_rel<SV>(b, depth); });
 }
 
 void hc_roundtrip(const uint64_t pos[6], uint64_t out[6])

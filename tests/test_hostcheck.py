@@ -1,6 +1,6 @@
 """The product's move generator (movegen.cuh), compiled for the host, against
-the oracle: legal-move counts, generated children and perft, for both slider
-variants.  Runs without a GPU."""
+the oracle: legal-move counts, generated children and perft, for every slider
+variant.  Runs without a GPU."""
 import ctypes
 import os
 import random
@@ -20,7 +20,7 @@ def hc():
     src = [os.path.join(HC_DIR, "hostcheck.cpp"), os.path.join(ROOT, "perft_gpu_b200", "csrc", "tables.cpp")]
     hdr = os.path.join(ROOT, "perft_gpu_b200", "csrc", "movegen.cuh")
     if not os.path.exists(HC_LIB) or any(os.path.getmtime(s) > os.path.getmtime(HC_LIB) for s in src + [hdr]):
-        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", HC_LIB] + src, check=True)
+        subprocess.run(["g++", "-O2", "-std=c++20", "-fPIC", "-shared", "-o", HC_LIB] + src, check=True)
     lib = ctypes.CDLL(HC_LIB)
     lib.hc_count.restype = ctypes.c_uint32
     lib.hc_children.restype = ctypes.c_uint32
@@ -35,7 +35,11 @@ def _children(hc, pos, sv):
     return sorted(tuple(buf[6 * i:6 * i + 6]) for i in range(n))
 
 
-@pytest.mark.parametrize("sv", [0, 1, 4], ids=["kogge", "magic", "hybrid"])
+SV_ALL = [0, 1, 2, 3, 4]
+SV_IDS = ["kogge", "magic", "kogge_fma", "kogge_split", "hybrid"]
+
+
+@pytest.mark.parametrize("sv", SV_ALL, ids=SV_IDS)
 def test_golden_perft(hc, golden, sv):
     for e in golden:
         p = P6(*[int(h, 16) for h in e["pos48"]])
@@ -44,7 +48,7 @@ def test_golden_perft(hc, golden, sv):
                 assert hc.hc_perft(p, int(d), sv) == int(c), (e["name"], d)
 
 
-@pytest.mark.parametrize("sv", [0, 1], ids=["kogge", "magic"])
+@pytest.mark.parametrize("sv", SV_ALL, ids=SV_IDS)
 def test_counts_and_children_vs_oracle(hc, oracle, sv):
     rng = random.Random(3 + sv)
     start = oracle.fen_to_pos("rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1")
@@ -68,3 +72,21 @@ def test_relative_roundtrip(hc, golden):
         p = P6(*[int(h, 16) for h in e["pos48"]])
         hc.hc_roundtrip(p, out)
         assert list(out) == list(p), e["name"]
+
+
+@pytest.mark.parametrize("sv", SV_ALL, ids=SV_IDS)
+def test_stratified_batch_sample_vs_oracle(hc, oracle, sv):
+    """The benchmark batch's special-rule strata (legal en-passant captures,
+    pawns on the 7th rank, castling rights) through the product's move
+    generator on the host: child sets and perft(2) against the oracle."""
+    import perft_gpu_b200 as pg
+    from perft_gpu_b200 import workloads
+    pos, _ = workloads.batch_positions(n=300, seed=17)
+    f = np.array([pg.features(p) for p in pos])
+    assert (f & pg.FEATURE_EP != 0).sum() >= 30
+    for p in pos:
+        pp = P6(*[int(x) for x in p])
+        kids = oracle.children(p)
+        assert hc.hc_count(pp, sv) == len(kids)
+        assert _children(hc, p, sv) == sorted(tuple(int(x) for x in k) for k in kids)
+        assert hc.hc_perft(pp, 2, sv) == oracle.perft(p, 2)

@@ -126,3 +126,22 @@ def test_oracle_vs_reference_many_moves(oracle):
             counts.append(c)
         assert counts[0] == counts[1], fen
         assert counts[0][0] >= 94
+
+
+@needs_ref
+def test_oracle_vs_reference_stratified_batch():
+    """The benchmark batch's strata, where seeded playouts alone rarely reach
+    an en-passant capture (about 0.5% of them): oracle and reference agree on
+    perft 1-3 of a 200-position sample."""
+    import perft_gpu_b200 as pg
+    from perft_gpu_b200 import workloads
+    from tests._oracle import Oracle
+    oracle = Oracle(os.path.join(ROOT, "oracle", "liboracle.so"))
+    pos, _ = workloads.batch_positions(n=200, seed=29)
+    ep = 0
+    for p in pos:
+        ep += (pg.features(p) & pg.FEATURE_EP) != 0
+        pp = P6(*[int(x) for x in p])
+        for d in (1, 2, 3):
+            assert oracle.perft(p, d) == ref.ref_perft(pp, d), ([hex(int(x)) for x in p], d)
+    assert ep >= 20
