@@ -350,7 +350,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": cfg,
-        "leaves_per_step": leaves_per_step * ws, "counts_stable": stable,
+        "leaves_per_step": int(tot), "counts_stable": stable,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(pos.nbytes),
                 "d2h_bytes_per_step": int(8 * n)},
         "gpu_launches": int(st["leaf_launches"] + st["expand_launches"] + st["other_launches"]),
