@@ -26,6 +26,7 @@
 //       root move, then "Nodes searched: N".
 #include <chrono>
 #include <map>
+#include <signal.h>
 #include <stdio.h>
 #include <sys/wait.h>
 #include <unistd.h>
@@ -121,11 +122,23 @@ int divided_sharded(const std::string &fen, uint32_t depth, uint32_t split, int 
     std::vector<pid_t> pids;
     std::vector<FILE *> outs;
     const std::string dep = std::to_string(depth), spl = std::to_string(split), n = std::to_string(gpus);
+    // a failed start stops and reaps the shards already running
+    auto abandon = [&]() {
+        for (FILE *f : outs)
+            if (f) fclose(f);
+        for (pid_t pid : pids) kill(pid, SIGTERM);
+        for (pid_t pid : pids) waitpid(pid, nullptr, 0);
+        return PERFT_ERR_INTERNAL;
+    };
     for (int i = 0; i < gpus; i++) {
         int fd[2];
-        if (pipe(fd) != 0) return PERFT_ERR_INTERNAL;
+        if (pipe(fd) != 0) return abandon();
         const pid_t pid = fork();
-        if (pid < 0) return PERFT_ERR_INTERNAL;
+        if (pid < 0) {
+            close(fd[0]);
+            close(fd[1]);
+            return abandon();
+        }
         if (pid == 0) {
             dup2(fd[1], 1);
             close(fd[0]);
