@@ -201,9 +201,12 @@ int perft_result_store_stats(uint64_t *entries, uint64_t *hits, uint64_t *append
 /* Records mode (launcher.h:1579-1695): each line of in_path is a FEN ending
  * with an occurrence count; "<line> <perft> <perft*count>" is appended to
  * in_path.op.  Lines already in the output are skipped (resume): the k-th
- * output line belongs to the k-th non-empty input line (empty lines are
- * neither searched nor counted).  Lines are read up to 2047 characters.
- * batch 0 means 4096 records per GPU batch. */
+ * complete output line belongs to the k-th non-empty input line (empty
+ * lines are neither searched nor counted); a torn last output line, left by
+ * a run stopped in the middle of a write, is cut off and its record searched
+ * again.  Input lines are read up to 2047 characters.  batch 0 means 4096
+ * records per GPU batch.  PERFT_ERR_IO: the output cannot be read, opened
+ * or written. */
 int perft_records(const char *in_path, uint32_t depth, uint32_t batch, uint64_t *records_done);
 
 /* ------------------------------------------------------- host utilities */

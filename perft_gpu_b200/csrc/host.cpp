@@ -647,23 +647,51 @@ int perft_result_store_stats(uint64_t *entries, uint64_t *hits, uint64_t *append
 // appended to "<in_path>.op".  Lines already present in the output are
 // skipped, so an interrupted run resumes where it stopped.  Lines are
 // searched in GPU batches of `batch` records.
+// Records finished by an earlier run: the complete ('\n'-terminated) lines
+// of the output file, whatever their length.  A torn last line (a run
+// stopped in the middle of a write) is cut off, so its record is searched
+// again instead of being skipped.
+static int finished_records(const std::string &opPath, size_t *done)
+{
+    *done = 0;
+    FILE *fo = fopen(opPath.c_str(), "rb");
+    if (!fo) return PERFT_OK;  // no output yet
+    off_t size = 0, complete = 0;
+    char buf[1 << 16];
+    size_t got;
+    while ((got = fread(buf, 1, sizeof buf, fo)) > 0) {
+        for (size_t i = 0; i < got; i++) {
+            if (buf[i] == '\n') {
+                (*done)++;
+                complete = size + (off_t)i + 1;
+            }
+        }
+        size += (off_t)got;
+    }
+    const bool failed = ferror(fo) != 0;
+    fclose(fo);
+    if (failed) return PERFT_ERR_IO;
+    if (complete != size && truncate(opPath.c_str(), complete) != 0) return PERFT_ERR_IO;
+    return PERFT_OK;
+}
+
 static int records_impl(const char *in_path, uint32_t depth, uint32_t batch, uint64_t *records_done)
 {
     if (!in_path || depth > 20) return PERFT_ERR_INVALID_ARG;
     if (!batch) batch = 4096;
+    if (records_done) *records_done = 0;
     FILE *fin = fopen(in_path, "r");
     if (!fin) return PERFT_ERR_NOT_FOUND;
     const std::string opPath = std::string(in_path) + ".op";
     size_t already = 0;
-    if (FILE *fo = fopen(opPath.c_str(), "r")) {
-        char buf[2048];
-        while (fgets(buf, sizeof buf, fo)) already++;
-        fclose(fo);
+    if (const int frc = finished_records(opPath, &already); frc != PERFT_OK) {
+        fclose(fin);
+        return frc;
     }
     FILE *fout = fopen(opPath.c_str(), "a");
     if (!fout) {
         fclose(fin);
-        return PERFT_ERR_INVALID_ARG;
+        return PERFT_ERR_IO;
     }
     std::vector<std::string> lines;
     std::vector<u64> pos, occ;
@@ -679,7 +707,7 @@ static int records_impl(const char *in_path, uint32_t depth, uint32_t batch, uin
         for (u32 i = 0; i < n; i++)
             fprintf(fout, "%s %llu %llu\n", lines[i].c_str(), (unsigned long long)out[i],
                     (unsigned long long)(out[i] * occ[i]));
-        fflush(fout);
+        if (fflush(fout) != 0 || ferror(fout)) return PERFT_ERR_IO;
         done += n;
         lines.clear();
         pos.clear();
