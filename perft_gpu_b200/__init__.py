@@ -114,7 +114,13 @@ def _load():
         raise ImportError(
             f"{LIB_PATH} is missing: build it with `python -m perft_gpu_b200.build` "
             "(the engine has no CPU fallback)")
-    lib = ctypes.CDLL(LIB_PATH)
+    return _bind(ctypes.CDLL(LIB_PATH), require_all=True)
+
+
+def _bind(lib, require_all: bool = False):
+    """Sets the C signatures of include/perft_b200.h on a loaded library.
+    Every entry point must exist unless require_all is False (a library
+    exporting part of the interface)."""
     P = ctypes.POINTER
     u64p = P(ctypes.c_uint64)
     sig = {
@@ -158,6 +164,8 @@ def _load():
         "perft_records": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, u64p]),
     }
     for name, (res, args) in sig.items():
+        if not require_all and not hasattr(lib, name):
+            continue
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args

@@ -11,9 +11,12 @@
 #include <unordered_map>
 #include <vector>
 
+#include <errno.h>
+#include <fcntl.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/file.h>
 #include <unistd.h>
 
 #include "../../include/perft_b200.h"
@@ -199,11 +202,65 @@ struct StoreKeyHash {
 struct ResultStore {
     std::mutex mu;
     bool open = false;
-    FILE *f = nullptr;
+    int fd = -1;  // append-only descriptor of the backing file, or -1
     std::unordered_map<StoreKey, u64, StoreKeyHash> map;
     u64 hits = 0, appended = 0;
 };
 ResultStore g_store;
+
+// Exclusive advisory lock on a store file for one scope.  Processes sharing
+// a store (the shard processes of a multi-GPU run) take it around every
+// append and around the open-time header write and tail repair, so no
+// process sees another's half-written batch.
+struct FileLock {
+    int fd;
+    bool ok;
+    explicit FileLock(int f) : fd(f)
+    {
+        int r;
+        do {
+            r = flock(fd, LOCK_EX);
+        } while (r != 0 && errno == EINTR);
+        ok = r == 0;
+    }
+    ~FileLock()
+    {
+        if (ok) flock(fd, LOCK_UN);
+    }
+};
+
+bool write_all(int fd, const void *buf, size_t len)
+{
+    const char *p = (const char *)buf;
+    while (len) {
+        const ssize_t w = write(fd, p, len);
+        if (w < 0) {
+            if (errno == EINTR) continue;
+            return false;
+        }
+        p += w;
+        len -= (size_t)w;
+    }
+    return true;
+}
+
+// Reads up to len bytes at off; returns the bytes read (short only at end
+// of file) or -1.
+ssize_t read_at(int fd, void *buf, size_t len, off_t off)
+{
+    char *p = (char *)buf;
+    size_t got = 0;
+    while (got < len) {
+        const ssize_t r = pread(fd, p + got, len - got, off + (off_t)got);
+        if (r < 0) {
+            if (errno == EINTR) continue;
+            return -1;
+        }
+        if (r == 0) break;
+        got += (size_t)r;
+    }
+    return (ssize_t)got;
+}
 
 // Looks up every board of `ids` at `depth`; found ones go to counts and are
 // removed from ids.
@@ -240,9 +297,18 @@ int store_add(const Frontier &f, u32 depth, const u32 *ids, const u64 *vals, u32
         r.check = record_check(r);
         recs.push_back(r);
     }
-    if (g_store.f && !recs.empty()) {
-        if (fwrite(recs.data(), sizeof(StoreRecord), recs.size(), g_store.f) != recs.size() || fflush(g_store.f))
+    if (g_store.fd >= 0 && !recs.empty()) {
+        // one write of whole records at the end of the file (O_APPEND) under
+        // the file lock; a failed write is cut back so that later appends,
+        // from this or another process, stay on record boundaries
+        FileLock lock(g_store.fd);
+        if (!lock.ok) return PERFT_ERR_IO;
+        const off_t end = lseek(g_store.fd, 0, SEEK_END);
+        if (end < 0) return PERFT_ERR_IO;
+        if (!write_all(g_store.fd, recs.data(), recs.size() * sizeof(StoreRecord))) {
+            if (ftruncate(g_store.fd, end) != 0) { /* the next open drops the torn tail */ }
             return PERFT_ERR_IO;
+        }
         g_store.appended += recs.size();
     }
     return PERFT_OK;
@@ -577,8 +643,8 @@ static int deep_frontier_impl(const perft_pos48 *pos, uint32_t depth, uint32_t s
 static int store_open_impl(const char *path)
 {
     std::lock_guard<std::mutex> lk(g_store.mu);
-    if (g_store.f) fclose(g_store.f);
-    g_store.f = nullptr;
+    if (g_store.fd >= 0) close(g_store.fd);
+    g_store.fd = -1;
     g_store.map.clear();
     g_store.hits = g_store.appended = 0;
     g_store.open = false;
@@ -586,37 +652,49 @@ static int store_open_impl(const char *path)
         g_store.open = true;
         return PERFT_OK;
     }
-    FILE *f = fopen(path, "r+b");
-    if (!f) f = fopen(path, "w+b");
-    if (!f) return PERFT_ERR_IO;
-    char head[64];
-    const size_t got = fread(head, 1, sizeof head, f);
-    if (got == 0) {
-        memset(head, 0, sizeof head);
-        memcpy(head, STORE_MAGIC, sizeof STORE_MAGIC);
-        if (fseek(f, 0, SEEK_SET) || fwrite(head, 1, sizeof head, f) != sizeof head || fflush(f)) {
-            fclose(f);
-            return PERFT_ERR_IO;
-        }
-    } else if (got != sizeof head || memcmp(head, STORE_MAGIC, sizeof STORE_MAGIC) != 0) {
-        fclose(f);
-        return PERFT_ERR_IO;
-    }
-    long good = (long)sizeof head;
-    StoreRecord r;
-    while (fread(&r, sizeof r, 1, f) == 1 && record_check(r) == r.check) {
-        BoardKey b;
-        memcpy(b.w, r.w, sizeof b.w);
-        g_store.map[StoreKey{b, r.depth}] = r.count;
-        good += (long)sizeof r;
-    }
-    // drop a torn or corrupt tail so that appends continue after the last good record
-    if (fflush(f) || ftruncate(fileno(f), good) || fseek(f, good, SEEK_SET)) {
-        fclose(f);
+    const int fd = open(path, O_RDWR | O_CREAT | O_APPEND | O_CLOEXEC, 0644);
+    if (fd < 0) return PERFT_ERR_IO;
+    auto fail = [&]() {
+        close(fd);
         g_store.map.clear();
         return PERFT_ERR_IO;
+    };
+    {
+        FileLock lock(fd);
+        if (!lock.ok) return fail();
+        char head[64];
+        const ssize_t got = read_at(fd, head, sizeof head, 0);
+        if (got == 0) {
+            memset(head, 0, sizeof head);
+            memcpy(head, STORE_MAGIC, sizeof STORE_MAGIC);
+            if (!write_all(fd, head, sizeof head)) return fail();
+        } else if (got != (ssize_t)sizeof head || memcmp(head, STORE_MAGIC, sizeof STORE_MAGIC) != 0) {
+            return fail();
+        }
+        off_t good = (off_t)sizeof head;
+        std::vector<StoreRecord> buf(4096);
+        for (bool more = true; more;) {
+            const ssize_t r = read_at(fd, buf.data(), buf.size() * sizeof(StoreRecord), good);
+            if (r < 0) return fail();
+            const size_t k = (size_t)r / sizeof(StoreRecord);
+            more = k == buf.size();
+            for (size_t i = 0; i < k; i++) {
+                const StoreRecord &rec = buf[i];
+                if (record_check(rec) != rec.check) {
+                    more = false;
+                    break;
+                }
+                BoardKey b;
+                memcpy(b.w, rec.w, sizeof b.w);
+                g_store.map[StoreKey{b, rec.depth}] = rec.count;
+                good += (off_t)sizeof rec;
+            }
+        }
+        // drop a torn or corrupt tail so that appends continue after the last good record
+        const off_t size = lseek(fd, 0, SEEK_END);
+        if (size < 0 || (size > good && ftruncate(fd, good) != 0)) return fail();
     }
-    g_store.f = f;
+    g_store.fd = fd;
     g_store.open = true;
     return PERFT_OK;
 }
@@ -625,8 +703,8 @@ int perft_result_store_close(void)
 {
     std::lock_guard<std::mutex> lk(g_store.mu);
     int rc = PERFT_OK;
-    if (g_store.f && fclose(g_store.f)) rc = PERFT_ERR_IO;
-    g_store.f = nullptr;
+    if (g_store.fd >= 0 && close(g_store.fd) != 0) rc = PERFT_ERR_IO;
+    g_store.fd = -1;
     g_store.map.clear();
     g_store.open = false;
     return rc;
