@@ -2,10 +2,13 @@
 // divided and deep perft, shards, the result store, records mode, FEN and
 // move utilities) linked against a stand-in for the GPU engine that counts
 // with the product's move generator compiled for the host.  The CPU test
-// suite drives those paths end to end through it; it is not part of the
+// suite drives those paths, and the perft_gpu program (cli.cpp) linked
+// against this library, end to end through it; it is not part of the
 // product library, which has no CPU path.
 #include <atomic>
 #include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
 
 #include "../../include/perft_b200.h"
 #include "../../perft_gpu_b200/csrc/movegen.cuh"
@@ -88,5 +91,37 @@ void hostapi_fail_after(long long batches, int status)
 const char *perft_status_string(int status)
 {
     return status == PERFT_OK ? "ok" : "error (host test build)";
+}
+
+// Engine lifecycle and the single-position call, for the command-line
+// program built against this library.  HOSTAPI_FAIL_DEVICE=<d> makes every
+// engine batch of a process initialised on device d fail with
+// PERFT_ERR_CUDA (the shard processes of a split run get device = shard).
+void perft_config_default(perft_config *cfg)
+{
+    if (!cfg) return;
+    memset(cfg, 0, sizeof *cfg);
+    cfg->sliders_expand = PERFT_SLIDERS_AUTO;
+    cfg->sliders_leaf = PERFT_SLIDERS_AUTO;
+}
+
+int perft_init(const perft_config *cfg)
+{
+    build_tables();
+    const char *fail = getenv("HOSTAPI_FAIL_DEVICE");
+    if (fail && cfg && cfg->device == atoi(fail)) hostapi_fail_after(0, PERFT_ERR_CUDA);
+    return PERFT_OK;
+}
+
+int perft_shutdown(void)
+{
+    return PERFT_OK;
+}
+
+int perft(const perft_pos48 *pos, uint32_t depth, uint64_t *out)
+{
+    if (!pos || !out || depth > 20) return PERFT_ERR_INVALID_ARG;
+    const uint8_t d = (uint8_t)depth;
+    return engine_batch_host(pos->bb, &d, 1, out);
 }
 }

@@ -213,3 +213,97 @@ def test_deep_argument_checks(api, oracle):
     with pytest.raises(pg.PerftError) as ei:
         pg.deep(bad, 3, 1)
     assert ei.value.status == pg.PERFT_ERR_INVALID_ARG
+
+
+# ------------------------------------------------- the perft_gpu program
+CLI_HOST = os.path.join(API_DIR, "perft_gpu_host")
+CLI_SRC = os.path.join(ROOT, "perft_gpu_b200", "csrc", "cli.cpp")
+
+
+@pytest.fixture(scope="module")
+def cli():
+    """cli.cpp linked against the host test library."""
+    build_hostapi()
+    if not os.path.exists(CLI_HOST) or os.path.getmtime(CLI_HOST) < max(os.path.getmtime(CLI_SRC),
+                                                                         os.path.getmtime(API_LIB)):
+        subprocess.run(["g++", "-O2", "-std=c++17", "-o", CLI_HOST, CLI_SRC, "-L", API_DIR, "-lhostapi",
+                        "-Wl,-rpath,$ORIGIN"], check=True)
+    return CLI_HOST
+
+
+def run_cli(cli, *args, env=None, stdin=None):
+    e = {k: v for k, v in os.environ.items() if not k.startswith(("PERFT_", "HOSTAPI_"))}
+    e.update(env or {})
+    return subprocess.run([cli, *args], capture_output=True, text=True, timeout=120, env=e, input=stdin)
+
+
+def parse_cli(out):
+    totals, div = {}, {}
+    for line in out.splitlines():
+        if line.startswith("Perft("):
+            totals[int(line[6:8])] = int(line.split(":")[1].split(",")[0])
+        elif len(line.split()) == 2:
+            m, c = line.split()
+            div[m] = int(c)
+    return totals, div
+
+
+def test_cli_lines_divided_and_sharded(cli, golden):
+    counts = next(e for e in golden if e["name"] == "initial_position")["counts"]
+    r = run_cli(cli, "startpos", "5")
+    assert r.returncode == 0, r.stderr
+    assert parse_cli(r.stdout)[0] == {d: counts[str(d)] for d in (3, 4, 5)}
+    outs = []
+    for gpus in ("1", "3"):
+        r = run_cli(cli, "startpos", "5", gpus, env={"PERFT_DIVIDED_DEPTH": "3"})
+        assert r.returncode == 0, r.stderr
+        totals, div = parse_cli(r.stdout)
+        assert totals == {d: counts[str(d)] for d in (3, 4, 5)}
+        assert len(div) == 20 and sum(div.values()) == counts["5"]
+        outs.append([line for line in r.stdout.splitlines() if not line.startswith("Perft(")])
+    assert outs[0] == outs[1]  # shard processes reproduce the one-process divided lines
+
+
+def test_cli_shards_share_one_store(cli, api, tmp_path):
+    path = str(tmp_path / "cli.store")
+    env = {"PERFT_DIVIDED_DEPTH": "3", "PERFT_STORE": path}
+    first = run_cli(cli, "startpos", "5", "3", env=env)
+    assert first.returncode == 0, first.stderr
+    size = os.path.getsize(path)
+    again = run_cli(cli, "startpos", "5", "3", env=env)
+    assert again.returncode == 0, again.stderr
+    assert parse_cli(again.stdout) == parse_cli(first.stdout)
+    assert os.path.getsize(path) == size  # the second run found every board and appended nothing
+    pg.store_open(path)
+    start = pg.fen_to_pos(pg.START_FEN)
+    assert pg.store_stats()["entries"] == pg.deep_frontier(start, 4, 1)[0] + pg.deep_frontier(start, 5, 1)[0]
+
+
+def test_cli_failed_shard_fails_the_run(cli):
+    """One shard process whose engine calls fail: the run reports an error
+    and exits non-zero instead of printing a partial count."""
+    r = run_cli(cli, "startpos", "5", "3", env={"PERFT_DIVIDED_DEPTH": "3", "HOSTAPI_FAIL_DEVICE": "1"})
+    assert r.returncode != 0
+    assert "shard 1 failed" in r.stderr
+    assert "Perft(04)" not in r.stdout and "Perft(05)" not in r.stdout
+
+
+def test_cli_records_and_uci(cli, tmp_path, oracle):
+    src, pos, occ = _records(tmp_path, n=6)
+    r = run_cli(cli, "--records", src, "3")
+    assert r.returncode == 0, r.stderr
+    lines = open(src + ".op").read().splitlines()
+    assert [int(line.rsplit(" ", 2)[1]) for line in lines] == [oracle.perft(p, 3) for p in pos]
+    script = "uci\nisready\nposition startpos moves e2e4 c7c5 g1f3\ngo perft 3\nquit\n"
+    r = run_cli(cli, "--uci", stdin=script)
+    assert r.returncode == 0, r.stderr
+    p = pg.position_from_moves(pg.START_FEN, ["e2e4", "c7c5", "g1f3"])
+    div, nodes = {}, None
+    for line in r.stdout.splitlines():
+        if line.startswith("Nodes searched:"):
+            nodes = int(line.split(":")[1])
+        elif ": " in line and not line.startswith("info"):
+            m, c = line.split(": ")
+            div[m] = int(c)
+    assert nodes == oracle.perft(p, 3)
+    assert sorted(div.values()) == sorted(oracle.perft(c, 2) for c in oracle.children(p))
