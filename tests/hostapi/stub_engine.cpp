@@ -42,6 +42,7 @@ u64 perft_host(const Board &b, u32 depth)
 std::atomic<u64> g_batches{0}, g_positions{0};
 std::atomic<long long> g_fail_after{-1};  // batches left before an injected failure; -1 never
 std::atomic<int> g_fail_status{PERFT_ERR_CUDA};
+std::atomic<u64> g_scale{1};  // every count is multiplied by this (totals beyond 64 bits on small trees)
 }  // namespace
 
 int pg::engine_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *out)
@@ -52,7 +53,7 @@ int pg::engine_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *out
     if (left > 0) g_fail_after.store(left - 1);
     for (u32 i = 0; i < n; i++) {
         if (depths[i] > 20) return PERFT_ERR_INVALID_ARG;
-        out[i] = perft_host(from_pos48(pos + 6ull * i), depths[i]);
+        out[i] = perft_host(from_pos48(pos + 6ull * i), depths[i]) * g_scale.load();
     }
     g_batches += 1;
     g_positions += n;
@@ -88,6 +89,13 @@ void hostapi_fail_after(long long batches, int status)
     g_fail_after = batches;
 }
 
+// Multiplies every count by `factor` (1 restores true counts): a small tree
+// then stands for one whose totals need more than 64 bits.
+void hostapi_scale(uint64_t factor)
+{
+    g_scale = factor;
+}
+
 const char *perft_status_string(int status)
 {
     return status == PERFT_OK ? "ok" : "error (host test build)";
@@ -96,7 +104,8 @@ const char *perft_status_string(int status)
 // Engine lifecycle and the single-position call, for the command-line
 // program built against this library.  HOSTAPI_FAIL_DEVICE=<d> makes every
 // engine batch of a process initialised on device d fail with
-// PERFT_ERR_CUDA (the shard processes of a split run get device = shard).
+// PERFT_ERR_CUDA (the shard processes of a split run get device = shard);
+// HOSTAPI_SCALE=<k> multiplies every count by k.
 void perft_config_default(perft_config *cfg)
 {
     if (!cfg) return;
@@ -110,6 +119,7 @@ int perft_init(const perft_config *cfg)
     build_tables();
     const char *fail = getenv("HOSTAPI_FAIL_DEVICE");
     if (fail && cfg && cfg->device == atoi(fail)) hostapi_fail_after(0, PERFT_ERR_CUDA);
+    if (const char *k = getenv("HOSTAPI_SCALE")) hostapi_scale(strtoull(k, nullptr, 10));
     return PERFT_OK;
 }
 

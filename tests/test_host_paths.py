@@ -32,6 +32,7 @@ def bind_hostapi():
     lib = pg._bind(ctypes.CDLL(build_hostapi()))
     lib.hostapi_counters.argtypes = [ctypes.POINTER(ctypes.c_uint64)] * 2
     lib.hostapi_fail_after.argtypes = [ctypes.c_longlong, ctypes.c_int]
+    lib.hostapi_scale.argtypes = [ctypes.c_uint64]
     lib.hostapi_init()
     return lib
 
@@ -41,9 +42,11 @@ def api(monkeypatch):
     lib = bind_hostapi()
     monkeypatch.setattr(pg, "_lib_handle", lib)
     lib.hostapi_fail_after(-1, 0)
+    lib.hostapi_scale(1)
     lib.hostapi_reset_counters()
     yield lib
     lib.hostapi_fail_after(-1, 0)
+    lib.hostapi_scale(1)
     pg.store_close()
 
 
@@ -307,3 +310,39 @@ def test_cli_records_and_uci(cli, tmp_path, oracle):
             div[m] = int(c)
     assert nodes == oracle.perft(p, 3)
     assert sorted(div.values()) == sorted(oracle.perft(c, 2) for c in oracle.children(p))
+
+
+U64_MAX = (1 << 64) - 1
+
+
+def test_totals_beyond_64_bits(api, oracle):
+    """Counts scaled so that every per-move subtotal fits 64 bits but the
+    total does not: exact subtotals and an exact wide total.  Scaled further,
+    a subtotal itself overflows and the call fails with no subtotals."""
+    start = pg.fen_to_pos(pg.START_FEN)
+    total, div = pg.deep(start, 4, 1)
+    k = U64_MAX // max(div.values())
+    assert k * total > U64_MAX
+    api.hostapi_scale(k)
+    wide, wdiv = pg.deep(start, 4, 1)
+    assert wdiv == {m: c * k for m, c in div.items()} and wide == k * total
+    # every frontier board's count still fits; the largest per-move sum does not
+    biggest_board = max(oracle.perft(g, 2) for c in oracle.children(start) for g in oracle.children(c))
+    k2 = U64_MAX // biggest_board
+    assert max(div.values()) * k2 > U64_MAX
+    api.hostapi_scale(k2)
+    with pytest.raises(pg.PerftError) as ei:
+        pg.deep(start, 4, 1)
+    assert ei.value.status == pg.PERFT_ERR_OVERFLOW
+
+
+def test_cli_prints_wide_totals(cli, golden, oracle):
+    counts = next(e for e in golden if e["name"] == "initial_position")["counts"]
+    start = pg.fen_to_pos(pg.START_FEN)
+    k = U64_MAX // max(oracle.perft(c, 3) for c in oracle.children(start))  # every depth-4 subtotal fits
+    for gpus in ("1", "2"):
+        r = run_cli(cli, "startpos", "4", gpus, env={"PERFT_DIVIDED_DEPTH": "3", "HOSTAPI_SCALE": str(k)})
+        assert r.returncode == 0, r.stderr
+        totals, div = parse_cli(r.stdout)
+        assert totals == {3: counts["3"] * k, 4: counts["4"] * k}
+        assert totals[4] > U64_MAX and sum(div.values()) == totals[4]
