@@ -346,3 +346,34 @@ def test_cli_prints_wide_totals(cli, golden, oracle):
         totals, div = parse_cli(r.stdout)
         assert totals == {3: counts["3"] * k, 4: counts["4"] * k}
         assert totals[4] > U64_MAX and sum(div.values()) == totals[4]
+
+
+def test_cli_uci_edge_cases(cli, oracle):
+    kiwi = "r3k2r/p1ppqpb1/bn2pnp1/3PN3/1p2P3/2N2Q1p/PPPBBPPP/R3K2R w KQkq - 0 1"
+    mate = "rnb1kbnr/pppp1ppp/8/4p3/6Pq/5P2/PPPPP2P/RNBQKBNR w KQkq - 1 3"
+    script = "\n".join([
+        "ucinewgame",
+        f"position fen {kiwi} moves e1g1 a8b8",
+        "d",
+        "position startpos moves e2e4 e2e5",   # second move illegal: position unchanged
+        "d",
+        "position fen not/a/fen",
+        "go perft 0",
+        "flip",
+        f"position fen {mate}",
+        "go perft 2",
+        "quit",
+    ]) + "\n"
+    r = run_cli(cli, "--uci", stdin=script)
+    assert r.returncode == 0, r.stderr
+    out = r.stdout.splitlines()
+    fens = [line[5:] for line in out if line.startswith("Fen: ")]
+    after = pg.position_from_moves(kiwi, ["e1g1", "a8b8"])
+    assert fens[0] == pg.pos_to_fen(after)
+    assert fens[1] == fens[0]
+    assert "info string illegal move e2e5" in out
+    assert "info string bad fen" in out
+    assert "info string bad depth" in out
+    assert "info string unknown command flip" in out
+    assert "Nodes searched: 0" in out  # checkmated: no moves, no leaves
+    assert oracle.perft(pg.fen_to_pos(mate), 1) == 0
