@@ -5,8 +5,9 @@ one deep position) dealt across ranks, and one small sum as the only exchange.
 This follows the reference's subtree parallelism (launcher.h:409-583: root
 children dealt to one host thread per GPU, the subtotals summed on the host).
 There are no cross-GPU loads: every rank searches its own subtrees with its own
-engine and transposition table, and the per-position or per-move counts (8
-bytes each) are summed with one all-reduce.
+engine and transposition table, and the per-position or per-move counts are
+summed with one all-reduce (16 bytes each: two 32-bit halves, exact at any
+size).
 
 The counting function is a parameter so that the dealing and reduction logic
 can run on CPU ranks (gloo) with any counter; by default it is the GPU engine.
@@ -30,13 +31,19 @@ def _world(group):
     return dist, dist.get_rank(group), dist.get_world_size(group)
 
 
-def _sum_u64(values: np.ndarray, dist, group, device) -> np.ndarray:
-    """Element-wise sum over ranks of a u64 vector (counts stay below 2^63)."""
+def _sum_u64(values: np.ndarray, dist, group, device) -> list:
+    """Element-wise sum over ranks of u64 counts, exact as Python ints at any
+    size (a per-move subtotal summed over shards may pass 2^64): each value
+    travels as its two 32-bit halves in int64 lanes, whose sums cannot
+    overflow for fewer than 2^31 ranks."""
     import torch
-    t = torch.from_numpy(np.ascontiguousarray(values, dtype=np.uint64).view(np.int64).copy()).to(device)
+    v = np.ascontiguousarray(values, dtype=np.uint64).reshape(-1)
+    halves = np.stack([v >> np.uint64(32), v & np.uint64(0xFFFFFFFF)]).astype(np.int64)
+    t = torch.from_numpy(halves).to(device)
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
-    return t.cpu().numpy().view(np.uint64)
+    hi, lo = t.cpu().numpy()
+    return [(int(h) << 32) + int(l) for h, l in zip(hi, lo)]
 
 
 def max_sum_over_ranks(maxes, sums, device="cpu", group=None):
@@ -66,7 +73,8 @@ def perft_batch_sharded(pos: np.ndarray, depths, counter=None, group=None, devic
     out = np.zeros(len(pos), dtype=np.uint64)
     if len(mine):
         out[mine] = np.asarray(counter(pos[mine], depths[mine]), dtype=np.uint64)
-    return _sum_u64(out, dist, group, device)
+    # one rank holds each position's count, so every sum fits 64 bits
+    return np.array(_sum_u64(out, dist, group, device), dtype=np.uint64)
 
 
 def deep_sharded(pos, depth: int, split_plies: int = 2, deep_fn=None, group=None, device="cpu"):
@@ -81,5 +89,5 @@ def deep_sharded(pos, depth: int, split_plies: int = 2, deep_fn=None, group=None
     _, div = deep_fn(pos, depth, split_plies, rank, world)
     moves = list(div.keys())
     summed = _sum_u64(np.array([div[m] for m in moves], dtype=np.uint64), dist, group, device)
-    result = {m: int(c) for m, c in zip(moves, summed)}
+    result = dict(zip(moves, summed))
     return sum(result.values()), result

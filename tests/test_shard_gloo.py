@@ -75,9 +75,12 @@ def _worker(rank, world, port, out_dir):
 
         total, div = shard.deep_sharded(mid, 3, 1, deep_fn=deep_fn)
         (tmax, emax), (leaves,) = shard.max_sum_over_ranks([1.0 + rank, 10.0 * rank], [100.0 * (rank + 1)])
+        # counts near and past 2^63 / 2^64 in the sum stay exact
+        wide = shard._sum_u64(np.array([2**63 + rank, 2**64 - 1 - rank, 2**32 - 1], dtype=np.uint64),
+                              dist, None, "cpu")
         with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
             json.dump({"batch": [int(x) for x in batch], "n_counted": len(seen), "total": total, "div": div,
-                       "tmax": tmax, "emax": emax, "leaves": leaves}, f)
+                       "tmax": tmax, "emax": emax, "leaves": leaves, "wide": [str(x) for x in wide]}, f)
     finally:
         dist.destroy_process_group()
 
@@ -106,6 +109,7 @@ def test_two_gloo_ranks_match_single_process(tmp_path, oracle):
         assert r["total"] == oracle.perft(mid, 3) == sum(want_div)
         assert [r["div"][f"m{i}"] for i in range(len(want_div))] == want_div
         assert (r["tmax"], r["emax"], r["leaves"]) == (2.0, 10.0, 300.0)
+        assert [int(x) for x in r["wide"]] == [2**64 + 1, 2**65 - 3, 2**33 - 2]
     # each position counted by exactly one rank
     assert sum(r["n_counted"] for r in res) == len(pos)
     assert abs(res[0]["n_counted"] - res[1]["n_counted"]) <= 1
