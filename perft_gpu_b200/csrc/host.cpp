@@ -211,21 +211,23 @@ ResultStore g_store;
 // Exclusive advisory lock on a store file for one scope.  Processes sharing
 // a store (the shard processes of a multi-GPU run) take it around every
 // append and around the open-time header write and tail repair, so no
-// process sees another's half-written batch.
+// process sees another's half-written batch.  On a file system without
+// lock support the scope runs unlocked: one process per store stays safe.
 struct FileLock {
     int fd;
-    bool ok;
+    bool locked = false, ok = false;
     explicit FileLock(int f) : fd(f)
     {
         int r;
         do {
             r = flock(fd, LOCK_EX);
         } while (r != 0 && errno == EINTR);
-        ok = r == 0;
+        locked = r == 0;
+        ok = locked || errno == ENOLCK || errno == EOPNOTSUPP || errno == ENOSYS;
     }
     ~FileLock()
     {
-        if (ok) flock(fd, LOCK_UN);
+        if (locked) flock(fd, LOCK_UN);
     }
 };
 
