@@ -377,3 +377,14 @@ def test_cli_uci_edge_cases(cli, oracle):
     assert "info string unknown command flip" in out
     assert "Nodes searched: 0" in out  # checkmated: no moves, no leaves
     assert oracle.perft(pg.fen_to_pos(mate), 1) == 0
+
+
+def test_divide_edges(api):
+    start = pg.fen_to_pos(pg.START_FEN)
+    assert pg.divide(start, 1) == {m: 1 for m in pg.legal_moves(start)}
+    for depth in (0, 40):
+        with pytest.raises(pg.PerftError) as ei:
+            pg.divide(start, depth)
+        assert ei.value.status == pg.PERFT_ERR_INVALID_ARG
+    mate = pg.fen_to_pos("rnb1kbnr/pppp1ppp/8/4p3/6Pq/5P2/PPPPP2P/RNBQKBNR w KQkq - 1 3")
+    assert pg.divide(mate, 3) == {} and pg.deep(mate, 3, 1) == (0, {})
