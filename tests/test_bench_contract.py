@@ -36,3 +36,21 @@ def test_reference_arm_other_workload():
     d = _run("--workload", "start", "--steps", "2", "--warmup", "1", "--cpu-seconds", "1")
     assert d["config"]["workload"].startswith("initial position, depth 5")
     assert d["steps"] == 2 and d["value"] > 0
+
+
+def test_reference_arm_other_ranks_exit_quietly():
+    """Under torchrun only rank 0 runs the reference arm and prints; the
+    other ranks exit 0 without work or output."""
+    env = dict(os.environ, WORLD_SIZE="2", RANK="1", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=120, cwd=ROOT,
+                       env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert not [x for x in r.stdout.splitlines() if x.startswith("{")]
+    env.update(RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--steps", "1", "--warmup", "0", "--cpu-seconds", "1"], capture_output=True, text=True,
+                       timeout=300, cwd=ROOT, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1 and lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"
