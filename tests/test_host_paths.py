@@ -388,3 +388,26 @@ def test_divide_edges(api):
         assert ei.value.status == pg.PERFT_ERR_INVALID_ARG
     mate = pg.fen_to_pos("rnb1kbnr/pppp1ppp/8/4p3/6Pq/5P2/PPPPP2P/RNBQKBNR w KQkq - 1 3")
     assert pg.divide(mate, 3) == {} and pg.deep(mate, 3, 1) == (0, {})
+
+
+def test_deep_property_random_positions(api, oracle):
+    """Seeded random positions, depths, splits and shard counts: the shards'
+    subtotals always sum to the oracle's perft, move by move."""
+    from hypothesis import HealthCheck, given, settings
+    from hypothesis import strategies as st
+
+    @settings(max_examples=40, deadline=None, derandomize=True,
+              suppress_health_check=[HealthCheck.function_scoped_fixture])
+    @given(seed=st.integers(0, 2**32 - 1), plies=st.integers(0, 60), depth=st.integers(1, 3),
+           split=st.integers(0, 3), n=st.integers(1, 4))
+    def check(seed, plies, depth, split, n):
+        pos = pg.random_playouts(seed=seed, n=1, min_plies=plies, max_plies=plies)[0]
+        acc = {}
+        for s in range(n):
+            _, div = pg.deep(pos, depth, split, shard=s, n_shards=n)
+            for m, c in div.items():
+                acc[m] = acc.get(m, 0) + c
+        assert sum(acc.values()) == oracle.perft(pos, depth)
+        assert sorted(acc.values()) == sorted(oracle.perft(c, depth - 1) for c in oracle.children(pos))
+
+    check()
