@@ -4,13 +4,25 @@
 Default workload: the batched perft of 4096 seeded, stratified playout
 positions at depths U[4,6] (one step = one perft_batch over the whole
 batch).  Other workloads: --workload start (initial position, depth 5,
-repeated), --workload deep (one 20-ply playout with >= 35 moves, depth 8).
+repeated), --workload deep (one 20-ply playout with >= 35 moves, depth 8),
+--workload tt (4 positions at depths 9-10 with a 2^30-entry table),
+--workload serve (Poisson serving trace).
+
+On one GPU the default run also measures the other configurations after the
+headline leg and reports them under "configs": the initial position at depth
+5, the depth-8 position, the transposition-table positions at depths 9-10,
+and the same 4096-position batch run one position per call (the
+batched/single ratio).  Counts are checked against the reference's own host
+perft (tests/golden/config_counts.json) where it has them.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Multi-GPU (torchrun): each rank searches its own 4096-position batch (seed
 offset by rank); there is no data-path collective, only a barrier and a
 max/sum reduction of the timings and counts.
+
+The workloads are read from perft_gpu_b200/data/workloads.npz (numpy only),
+so the reference arm's process never loads the engine library.
 
 Prints one JSON line (rank 0).
 """
@@ -129,51 +141,123 @@ def traffic_from_profiles(workload, items_per_launch):
 
 
 # ------------------------------------------------------------------ workloads
+WL_PATH = os.path.join(ROOT, "perft_gpu_b200", "data", "workloads.npz")
+GOLDEN_PATH = os.path.join(ROOT, "tests", "golden", "config_counts.json")
+
+
+def stored_workloads():
+    """The seeded workloads as plain arrays (numpy only: no engine library)."""
+    with np.load(WL_PATH) as z:
+        return {k: z[k] for k in z.files}
+
+
+def reference_counts():
+    """Counts of the reference's own host perft on the stored workloads, or None."""
+    if not os.path.exists(GOLDEN_PATH):
+        return None
+    with open(GOLDEN_PATH) as f:
+        return json.load(f)
+
+
+def reference_start_counts():
+    """The reference's perft of the initial position by depth (tests/golden/perft_golden.json)."""
+    path = os.path.join(ROOT, "tests", "golden", "perft_golden.json")
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        g = json.load(f)
+    for e in g["positions"]:
+        if e["name"] == "initial_position":
+            return {int(k): int(v) for k, v in e["counts"].items()}
+    return {}
+
+
+BATCH_DESC = ("batch{n}: {n} seeded playouts of 8-30 plies, stratified "
+              "(>=10% en passant, >=10% pawn on 7th, >=10% castling), depth U[4,6]")
+
+
 def make_workload(name, rank, positions=4096):
-    from perft_gpu_b200 import workloads as W
+    wl = stored_workloads()
     if name == "batch":
-        pos, depths = W.batch_positions(n=4096, seed=2026 + rank)
+        if rank == 0:
+            pos, depths = wl["batch_pos"], wl["batch_depths"]
+        else:
+            # other ranks' batches (GPU arm under torchrun only): generated
+            from perft_gpu_b200 import workloads as W
+            pos, depths = W.batch_positions(n=4096, seed=2026 + rank)
         pos, depths = pos[:positions], depths[:positions]
-        cfg = {"workload": f"batch{positions}: {positions} seeded playouts of 8-30 plies, stratified "
-                           "(>=10% en passant, >=10% pawn on 7th, >=10% castling), depth U[4,6]",
+        cfg = {"workload": BATCH_DESC.format(n=positions),
                "positions": positions, "depths": "U[4,6]", "seed": 2026 + rank}
         return pos, depths, cfg, "batch4096"
     if name == "start":
-        pos = np.repeat(W.start_position().reshape(1, 6), 1, axis=0)
+        pos = np.array([[0xFFFF, 0x00FF00000000FF0F, 0x4200000000000042, 0x2C0000000000002C,
+                         0x8900000000000089, 0x1000000000000010]], dtype=np.uint64)
         cfg = {"workload": "initial position, depth 5, no transposition table", "positions": 1,
                "depths": "5"}
         return pos, np.array([5], dtype=np.uint8), cfg, "start"
     if name == "deep":
-        pos = W.deep_position().reshape(1, 6)
         cfg = {"workload": "one seeded 20-ply playout with >=35 legal moves, depth 8, no TT",
                "positions": 1, "depths": "8"}
-        return pos, np.array([8], dtype=np.uint8), cfg, "deep"
+        return wl["deep_pos"].reshape(1, 6), np.array([8], dtype=np.uint8), cfg, "deep"
     raise SystemExit(f"unknown workload {name}")
 
 
 # ------------------------------------------------------------------ CPU arms
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _cpu_has_x86_64_v3():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    return {"avx2", "bmi1", "bmi2", "fma", "movbe", "abm"} <= flags
+    except OSError:
+        pass
+    return False
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def cpu_perft_lib():
-    """The reference's host perft when it was built (oracle/_ref), else the oracle port."""
-    ref = os.path.join(ROOT, "oracle", "_ref", "libperft_ref.so")
-    if os.path.exists(ref):
-        lib = ctypes.CDLL(ref)
-        lib.ref_init()
-        fn = lib.ref_perft_batch_mt
-        return "reference", fn
+    """The reference's host perft when it was built (oracle/_ref: the x86-64-v3
+    build on hosts with AVX2/BMI2, else the SSE4.2 build), else the oracle port."""
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    names = (["libperft_ref.so"] if _cpu_has_x86_64_v3() else []) + ["libperft_ref_sse42.so"]
+    for name in names:
+        path = os.path.join(ref_dir, name)
+        if os.path.exists(path):
+            lib = ctypes.CDLL(path)
+            lib.ref_init()
+            return "reference", lib.ref_perft_batch_mt, name
     orc = os.path.join(ROOT, "oracle", "liboracle.so")
     if not os.path.exists(orc):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"], check=True,
                        stdout=subprocess.DEVNULL)
     lib = ctypes.CDLL(orc)
     lib.oracle_init()
-    return "port", lib.oracle_perft_batch_mt
+    return "port", lib.oracle_perft_batch_mt, "liboracle.so"
 
 
 def cpu_sample(pos, depths, budget_s, expected=None, threads=None):
     """Runs the CPU perft over a bounded sample of the workload: a seeded
     random order of its positions, taken in groups until budget_s elapses."""
-    kind, fn = cpu_perft_lib()
-    threads = threads or os.cpu_count() or 1
+    kind, fn, libname = cpu_perft_lib()
+    threads = threads or host_threads()
     order = np.random.default_rng(123).permutation(len(pos))
     done, leaves, t0 = 0, 0, time.perf_counter()
     mismatches = 0
@@ -192,6 +276,7 @@ def cpu_sample(pos, depths, budget_s, expected=None, threads=None):
         group = min(group * 2, 128)
     el = time.perf_counter() - t0
     return {"value": leaves / el, "unit": UNIT, "cores": threads, "kind": kind,
+            "cpu": cpu_model(), "library": f"oracle/_ref/{libname}" if kind == "reference" else f"oracle/{libname}",
             "sample": f"{done} of {len(pos)} positions (seeded order) at their own depths, "
                       f"{leaves} leaves in {el:.1f} s",
             "mismatches_vs_gpu": mismatches if expected is not None else None}
@@ -215,13 +300,160 @@ def run_reference(args):
             "ms_per_step": None, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": last["cores"], "kind": last["kind"],
-                             "sample": last["sample"]},
+                             "cpu": last["cpu"], "library": last["library"], "sample": last["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
 # ------------------------------------------------------------------ GPU arm
+def single_form_step(pg, d_pos, depths, d_out):
+    """The plain one-position-per-launch form: each position is copied into one
+    fixed device slot and searched by its own perft_batch_device call (a fixed
+    slot lets the engine reuse its per-depth launch graphs)."""
+    import torch
+    n = len(depths)
+    slot = torch.zeros(6, dtype=torch.int64, device="cuda")
+    res = torch.zeros(1, dtype=torch.int64, device="cuda")
+
+    def step():
+        for i in range(n):
+            slot.copy_(d_pos[i])
+            pg.perft_batch_device(slot.data_ptr(), depths[i:i + 1], 1, res.data_ptr())
+            d_out[i:i + 1].copy_(res)
+    return step
+
+
+def device_timed(fn, steps, device):
+    """Device time (ms) of `steps` calls of fn, between CUDA events on torch's
+    current stream (the legacy default stream; the engine's stream is a
+    blocking stream, so the events bracket its work), with clocks sampled
+    during the region."""
+    import torch
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clk:
+        torch.cuda.synchronize()
+        s.record()
+        for _ in range(steps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+    return s.elapsed_time(e), clk.summary()
+
+
+def measure_configs(args, pg, device, d_pos, depths, batch_ms_per_step, golden):
+    """The other configurations on this GPU, after the headline leg: the
+    initial position at depth 5, the depth-8 position, the 4096-position batch
+    one position per call, and (last: it re-creates the engine with a 2^30-entry
+    table) the transposition-table positions at depths 9-10."""
+    import torch
+    wl = stored_workloads()
+    out = {}
+
+    # initial position, depth 5, no table: latency-bound, many steps
+    start, dstart, _, _ = make_workload("start", 0)
+    sp = torch.from_numpy(start.view(np.int64)).cuda()
+    so = torch.zeros(1, dtype=torch.int64, device="cuda")
+    fn = lambda: pg.perft_batch_device(sp.data_ptr(), dstart, 1, so.data_ptr())  # noqa: E731
+    for _ in range(20):
+        fn()
+    steps = 200
+    ms, clk = device_timed(fn, steps, device)
+    leaves = int(so.cpu().numpy().view(np.uint64)[0])
+    want = reference_start_counts().get(5)
+    e_ms, _ = device_timed(lambda: pg.perft(start[0], 5), steps, device)
+    out["start_d5"] = {"workload": "initial position, depth 5, no transposition table", "steps": steps,
+                       "ms_per_step": ms / steps, "value": leaves * steps / (ms / 1e3), "unit": UNIT,
+                       "leaves": leaves, "equals_reference": (leaves == want) if want else None,
+                       "e2e": {"value": leaves * steps / (e_ms / 1e3), "unit": UNIT,
+                               "h2d_bytes_per_step": 48, "d2h_bytes_per_step": 8},
+                       "clocks": clk}
+
+    # one position at depth 8, no table
+    dp = torch.from_numpy(wl["deep_pos"].reshape(1, 6).view(np.int64)).cuda()
+    do = torch.zeros(1, dtype=torch.int64, device="cuda")
+    d8 = np.array([8], dtype=np.uint8)
+    fn = lambda: pg.perft_batch_device(dp.data_ptr(), d8, 1, do.data_ptr())  # noqa: E731
+    fn()
+    steps = 2
+    pg.reset_stats()
+    ms, clk = device_timed(fn, steps, device)
+    st = pg.stats()
+    leaves = int(do.cpu().numpy().view(np.uint64)[0])
+    want = golden["deep"]["total"] if golden and "deep" in golden else None
+    out["deep_d8"] = {"workload": "one seeded 20-ply playout with >=35 legal moves, depth 8, no TT",
+                      "steps": steps, "ms_per_step": ms / steps, "value": leaves * steps / (ms / 1e3),
+                      "unit": UNIT, "leaves": leaves, "equals_reference": (leaves == want) if want else None,
+                      "leaf_share_of_step": st["leaf_ms"] / ms if ms > 0 else None,
+                      "chunked_levels": st["chunked_levels"], "clocks": clk}
+
+    # the same 4096-position batch, one position per call
+    n = len(depths)
+    so = torch.zeros(n, dtype=torch.int64, device="cuda")
+    step = single_form_step(pg, d_pos, depths, so)
+    ms, clk = device_timed(step, 1, device)
+    single = so.cpu().numpy().view(np.uint64)
+    want = np.array(golden["batch4096"]["counts"][:n], dtype=np.uint64) if golden else None
+    out["batch4096_single"] = {
+        "workload": BATCH_DESC.format(n=n) + ", one perft_batch_device call per position (fixed device slot)",
+        "steps": 1, "ms_per_step": ms, "value": float(single.sum()) / (ms / 1e3), "unit": UNIT,
+        "equals_reference": bool(np.array_equal(single, want)) if want is not None else None,
+        "batched_over_single": ms / batch_ms_per_step, "clocks": clk}
+
+    # transposition-table positions at depths 9-10 (2^30 entries), after the
+    # depth-8 check without and with the table against the reference
+    out["tt_d9_10"] = tt_leg(pg, device, wl, args, golden, timed_steps=1)
+    return out
+
+
+def tt_leg(pg, device, wl, args, golden, timed_steps=1, warmup=0):
+    """Depths 9-10 of the 4 table positions with a 2^tt_log2-entry table
+    (cleared before each step), after checking depth 8 with and without the
+    table against the reference's counts."""
+    import torch
+    pos = wl["tt_pos"]
+    depths = np.minimum(wl["tt_depths"], args.max_depth).astype(np.uint8)
+    pd = args.parity_depth
+    arena = int(args.arena_gb * (1 << 30))
+    pg.init(device=device, arena_bytes=arena)
+    t0 = time.perf_counter()
+    plain = pg.perft_batch(pos, pd)
+    t_plain = time.perf_counter() - t0
+    pg.init(device=device, arena_bytes=arena, tt_log2_entries=args.tt_log2)
+    t0 = time.perf_counter()
+    with_tt = pg.perft_batch(pos, pd)
+    t_tt = time.perf_counter() - t0
+    ref = None
+    if golden and "tt" in golden and pd == 8:
+        ref = [int(e["total"]) for e in golden["tt"]]
+    d_pos = torch.from_numpy(np.ascontiguousarray(pos).view(np.int64)).cuda()
+    d_out = torch.zeros(len(pos), dtype=torch.int64, device="cuda")
+    fn = lambda: pg.perft_batch_device(d_pos.data_ptr(), depths, len(pos), d_out.data_ptr())  # noqa: E731
+    total_ms, clk_all, counts = 0.0, [], None
+    for step in range(warmup + timed_steps):
+        pg.tt_clear()
+        pg.reset_stats()
+        ms, clk = device_timed(fn, 1, device)
+        if step >= warmup:
+            total_ms += ms
+            clk_all.append(clk)
+        counts = d_out.cpu().numpy().view(np.uint64).copy()
+    st = pg.stats()
+    leaves = int(counts.sum())
+    return {"workload": "4 seeded playouts of 12-24 plies, TT of 2^%d x 16 B, table cleared each step"
+                        % args.tt_log2,
+            "depths": depths.tolist(), "steps": timed_steps, "ms_per_step": total_ms / timed_steps,
+            "value": leaves * timed_steps / (total_ms / 1e3), "unit": UNIT + " (effective: leaves counted)",
+            "counts": [int(x) for x in counts],
+            "parity_depth%d" % pd: {"no_tt": [int(x) for x in plain], "tt": [int(x) for x in with_tt],
+                                    "tt_equals_no_tt": bool(np.array_equal(plain, with_tt)),
+                                    "equals_reference": (([int(x) for x in plain] == ref) and
+                                                         ([int(x) for x in with_tt] == ref)) if ref else None,
+                                    "no_tt_s": t_plain, "tt_s": t_tt},
+            "tt": {k: st[k] for k in ("tt_entries", "tt_probes", "tt_hits", "tt_duplicates", "tt_stores")},
+            "clocks": clk_all[-1] if clk_all else None}
+
+
 def run_ours(args):
     import torch
     import perft_gpu_b200 as pg
@@ -240,19 +472,14 @@ def run_ours(args):
     sliders = {"auto": pg.SLIDERS_AUTO, **{v: k for k, v in pg.SLIDER_NAMES.items()}}[args.sliders]
     pg.init(device=local, sliders_expand=sliders, sliders_leaf=sliders,
             arena_bytes=int(args.arena_gb * (1 << 30)))
+    tuning = [{k: v for k, v in e.items()} for e in pg.tuning()]
 
     n = len(pos)
     d_pos = torch.from_numpy(pos.view(np.int64)).cuda()
     d_out = torch.zeros(n, dtype=torch.int64, device="cuda")
 
     if args.form == "single":
-        # one position per call: the plain one-position-per-launch form
-        elem = d_pos.element_size() * 6
-
-        def step_device():
-            for i in range(n):
-                pg.perft_batch_device(d_pos.data_ptr() + i * elem, depths[i:i + 1], 1,
-                                      d_out.data_ptr() + i * d_out.element_size())
+        step_device = single_form_step(pg, d_pos, depths, d_out)
     else:
         def step_device():
             pg.perft_batch_device(d_pos.data_ptr(), depths, n, d_out.data_ptr())
@@ -335,6 +562,18 @@ def run_ours(args):
         "work_figures": {k: wf[k] for k in ("c_count", "c_make", "c_gen")},
     }
 
+    golden = reference_counts()
+    parity = None
+    if golden and args.workload == "batch" and rank == 0 and len(counts) <= len(golden["batch4096"]["counts"]):
+        want = np.array(golden["batch4096"]["counts"][:len(counts)], dtype=np.uint64)
+        parity = {"positions": int(len(counts)), "equal": int(np.count_nonzero(counts == want)),
+                  "reference": "oracle/_ref host perft, every position at its own depth "
+                               "(tests/golden/config_counts.json)"}
+
+    configs = None
+    if ws == 1 and args.workload == "batch" and args.form == "batch" and not args.no_configs:
+        configs = measure_configs(args, pg, local, d_pos, depths, ms_max / args.steps, golden)
+
     cpu = None
     if ws == 1 and not args.no_cpu:
         cpu = cpu_sample(pos, depths, args.cpu_seconds, expected=counts)
@@ -343,14 +582,14 @@ def run_ours(args):
     cfg.update({"form": "one perft call per position" if args.form == "single" else "one batched call",
                 "sliders": {"leaf": pg.SLIDER_NAMES.get(st["sliders_leaf"], "?"),
                             "interior": pg.SLIDER_NAMES.get(st["sliders_expand"], "?"),
-                            "chosen_by": args.sliders},
+                            "chosen_by": args.sliders, "per_depth": tuning},
                 "l2": "no flush: each step streams multi-GB level buffers through HBM (>> 126 MB L2)",
                 "parallelism": f"independent batches, {ws} GPU(s)"})
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": cfg,
-        "leaves_per_step": int(tot), "counts_stable": stable,
+        "leaves_per_step": int(tot), "counts_stable": stable, "counts_vs_reference": parity,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(pos.nbytes),
                 "d2h_bytes_per_step": int(8 * n)},
         "gpu_launches": int(st["leaf_launches"] + st["expand_launches"] + st["other_launches"]),
@@ -358,6 +597,8 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
     }
+    if configs is not None:
+        line["configs"] = configs
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -365,45 +606,19 @@ def run_ours(args):
 
 
 def run_tt(args):
-    """Transposition-table workload: 4 seeded playouts of 12-24 plies at
-    depths 9-10 with a 2^30-entry table; parity with the no-table engine is
-    checked at depth 8 first."""
+    """Transposition-table workload alone: 4 seeded playouts of 12-24 plies
+    at depths 9-10 with a 2^30-entry table; parity with the no-table engine
+    and with the reference is checked at depth 8 first."""
     import perft_gpu_b200 as pg
-    from perft_gpu_b200 import workloads as W
-    pos, depths = W.tt_positions()
-    depths = np.minimum(depths, args.max_depth).astype(np.uint8)
-    arena = int(args.arena_gb * (1 << 30))
-    pd = args.parity_depth
-    pg.init(device=0, arena_bytes=arena)
-    t0 = time.perf_counter()
-    d8_plain = pg.perft_batch(pos, pd)
-    t_plain = time.perf_counter() - t0
-    pg.init(device=0, arena_bytes=arena, tt_log2_entries=args.tt_log2)
-    t0 = time.perf_counter()
-    d8_tt = pg.perft_batch(pos, pd)
-    t_tt8 = time.perf_counter() - t0
-    times, counts = [], None
-    for step in range(args.warmup + args.steps):
-        pg.tt_clear()
-        pg.reset_stats()
-        t0 = time.perf_counter()
-        counts = pg.perft_batch(pos, depths)
-        el = time.perf_counter() - t0
-        if step >= args.warmup:
-            times.append(el)
-    st = pg.stats()
-    leaves = int(counts.sum())
+    import torch
+    torch.cuda.set_device(0)
+    r = tt_leg(pg, 0, stored_workloads(), args, reference_counts(), timed_steps=args.steps,
+               warmup=args.warmup)
     line = {"metric": "perft leaf nodes/s with transposition table (effective, bit-exact)",
-            "value": leaves / float(np.mean(times)), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True,
-            "dtype": "u64", "data": "synthetic",
-            "config": {"workload": "4 seeded playouts of 12-24 plies, TT of 2^%d x 16 B, table cleared each step"
-                                   % args.tt_log2, "depths": depths.tolist()},
-            "counts": [int(x) for x in counts],
-            "parity_depth%d" % pd: {"equal": bool(np.array_equal(d8_plain, d8_tt)), "no_tt_s": t_plain,
-                                    "tt_s": t_tt8, "counts": [int(x) for x in d8_plain]},
-            "tt": {k: st[k] for k in ("tt_entries", "tt_probes", "tt_hits", "tt_duplicates", "tt_stores")},
-            "timing": "host wall clock around the synchronous perft_batch call"}
+            "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": r["workload"], "depths": r["depths"]},
+            **{k: v for k, v in r.items() if k not in ("workload", "depths", "value", "ms_per_step", "steps")}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -462,6 +677,8 @@ def main():
     ap.add_argument("--arena-gb", type=float, default=0.0, help="level-buffer arena (0 = 85%% of free HBM)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations measured after the headline leg")
     ap.add_argument("--form", choices=["batch", "single"], default="batch",
                     help="batch workload: one batched call, or one call per position")
     ap.add_argument("--tt-log2", type=int, default=30, help="tt workload: table entries (log2)")

@@ -116,11 +116,15 @@ int perft_divide(const perft_pos48 *pos, uint32_t depth, char (*moves)[6], uint6
  * PERFT_NOALLOC_SCRATCH_BYTES compiled into the library, which every GPU
  * that loads the library keeps until the process exits.  Batches whose
  * levels do not fit it fail with PERFT_ERR_OUT_OF_MEMORY (use the arena
- * entry points for those).  All calls share the scratch; calls are
- * serialised by a lock and return after their GPU work has finished, since
- * overlapping calls would race on it.  The first call on a device uploads
- * the move tables and looks up the scratch address; make it before any
- * stream capture. */
+ * entry points for those).  All calls share the scratch, which keeps the
+ * last call's contents (each call clears what must start at zero); calls
+ * whose GPU work overlapped would race on it, so calls are serialised by a
+ * lock, and every call, a failing one included, waits for its stream before
+ * it returns: the call is synchronous.  The first call on a device does the
+ * set-up (uploads the move tables, looks up the scratch address with that
+ * device current); make that first call before any stream capture.  Later
+ * calls look the address up again and redo the set-up if the device's
+ * context was re-created (cudaDeviceReset). */
 #define PERFT_NOALLOC_SCRATCH_BYTES (32ull << 20)
 int perft_batch_noalloc(const perft_pos48 *d_pos, const uint8_t *depths, uint32_t n,
                         uint64_t *d_out, void *stream);
@@ -137,6 +141,10 @@ typedef struct perft_serve_config {
     uint64_t memory_bytes;   /* budget for resident frontiers (0: 90% of the free arena) */
     uint64_t step_items;     /* items a level may advance per iteration (0: 2^27) */
     uint32_t max_in_flight;  /* admitted queries at once (0: 4096, at most 65536) */
+    int32_t  use_tt;         /* 1 (default): frontier levels two plies above the leaves probe,
+                                de-duplicate and store into the engine's transposition table
+                                (perft_init with tt_log2_entries > 0), shared by every query
+                                and kept across queries; 0: no table */
 } perft_serve_config;
 
 typedef struct perft_serve_stats {
@@ -144,6 +152,9 @@ typedef struct perft_serve_stats {
     uint64_t iterations, launches;
     uint64_t memory_budget, memory_reserved, memory_peak;
     int      last_error;
+    /* table use by the server since perft_serve_start: nodes probed, answered
+     * from the table, merged with an identical node of the same level, stored */
+    uint64_t tt_probes, tt_hits, tt_merged, tt_stores;
 } perft_serve_stats;
 
 void perft_serve_config_default(perft_serve_config *cfg);
@@ -257,6 +268,22 @@ typedef struct perft_stats {
 } perft_stats;
 
 int perft_get_stats(perft_stats *out);
+
+/* Launch configuration in use per (ply kind, remaining depth): chosen by the
+ * per-depth autotuner at perft_init when the sliders are PERFT_SLIDERS_AUTO,
+ * else the configured variant with the largest tiles.  Entries: the
+ * count-only ply (remaining depth 2), then interior plies by remaining depth
+ * 3..N (deeper plies use entry N).  No counterpart in the reference, whose
+ * launch shape is fixed at compile time (switches.h:13-26). */
+typedef struct perft_tune_entry {
+    int    leaf;         /* 1: count-only last ply; 0: interior ply */
+    int    remaining;    /* remaining depth of the parent level */
+    int    sliders;      /* PERFT_SLIDERS_* variant */
+    int    tile_log2;    /* largest tile (log2 items); small levels use smaller tiles */
+    int    ctas_per_sm;  /* resident CTAs per SM; 0: all that fit */
+    double calib_ms;     /* median calibration time of this key; 0: not timed */
+} perft_tune_entry;
+int perft_get_tuning(perft_tune_entry *out, uint32_t cap, uint32_t *n);
 int perft_reset_stats(void);
 
 /* Empties the transposition table (entries stay valid across calls, since a

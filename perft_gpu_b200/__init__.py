@@ -100,13 +100,15 @@ class ServeConfig(ctypes.Structure):
         ("memory_bytes", ctypes.c_uint64),
         ("step_items", ctypes.c_uint64),
         ("max_in_flight", ctypes.c_uint32),
+        ("use_tt", ctypes.c_int32),
     ]
 
 
 class ServeStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "submitted", "completed", "in_flight", "queued", "iterations", "launches",
-        "memory_budget", "memory_reserved", "memory_peak")] + [("last_error", ctypes.c_int)]
+        "memory_budget", "memory_reserved", "memory_peak")] + [("last_error", ctypes.c_int)] + [
+        (n, ctypes.c_uint64) for n in ("tt_probes", "tt_hits", "tt_merged", "tt_stores")]
 
 
 def _load():
@@ -143,6 +145,7 @@ def _bind(lib, require_all: bool = False):
                                                  ctypes.c_uint32, ctypes.c_void_p]),
         "perft_position_features": (ctypes.c_int, [P(_Pos48), P(ctypes.c_uint32)]),
         "perft_get_stats": (ctypes.c_int, [P(PerftStats)]),
+        "perft_get_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, P(ctypes.c_uint32)]),
         "perft_reset_stats": (ctypes.c_int, []),
         "perft_tt_clear": (ctypes.c_int, []),
         "perft_serve_config_default": (None, [P(ServeConfig)]),
@@ -276,6 +279,23 @@ def stats() -> dict:
     return {name: getattr(s, name) for name, _ in PerftStats._fields_}
 
 
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("leaf", ctypes.c_int), ("remaining", ctypes.c_int), ("sliders", ctypes.c_int),
+                ("tile_log2", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("calib_ms", ctypes.c_double)]
+
+
+def tuning() -> list:
+    """The launch configuration per (ply kind, remaining depth) in use:
+    [{"ply": "leaf"|"interior", "remaining": r, "sliders": name, "tile": items,
+      "ctas_per_sm": k (0: all that fit), "calib_ms": ms}, ...]."""
+    buf = (TuneEntry * 32)()
+    n = ctypes.c_uint32(0)
+    _check(lib().perft_get_tuning(ctypes.cast(buf, ctypes.c_void_p), 32, ctypes.byref(n)), "perft_get_tuning")
+    return [{"ply": "leaf" if e.leaf else "interior", "remaining": e.remaining,
+             "sliders": SLIDER_NAMES.get(e.sliders, "?"), "tile": 1 << e.tile_log2,
+             "ctas_per_sm": e.ctas_per_sm, "calib_ms": e.calib_ms} for e in buf[:n.value]]
+
+
 def reset_stats() -> None:
     lib().perft_reset_stats()
 
@@ -334,10 +354,13 @@ def records(path: str, depth: int, batch: int = 4096) -> int:
 
 
 # ---------------------------------------------------------------- serving
-def serve_start(memory_bytes: int = 0, step_items: int = 0, max_in_flight: int = 0) -> None:
-    """Starts the continuous-batching server (after init)."""
+def serve_start(memory_bytes: int = 0, step_items: int = 0, max_in_flight: int = 0, use_tt: bool = True) -> None:
+    """Starts the continuous-batching server (after init).  With use_tt and an
+    engine table (init with tt_log2_entries), the server's frontier levels two
+    plies above the leaves probe, de-duplicate and store into that table."""
     cfg = ServeConfig()
     lib().perft_serve_config_default(ctypes.byref(cfg))
+    cfg.use_tt = 1 if use_tt else 0
     if memory_bytes:
         cfg.memory_bytes = memory_bytes
     if step_items:

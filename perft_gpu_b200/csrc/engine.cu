@@ -846,6 +846,44 @@ private:
     int gridTile[2][SV_COUNT] = {};
     bool trace = false;  // PERFT_TRACE=1: one stderr line per tile launch
 
+public:
+    // Launch configuration per (ply kind, remaining depth of the parent level):
+    // slider variant, largest tile (log2 items) and resident CTAs per SM.  The
+    // count-only ply always has remaining depth 2; interior plies have 3..20
+    // and use the entry of the nearest calibrated depth.
+    struct TuneCfg {
+        int sv = SV_KOGGE;
+        int cap = TILE_CAP_LOG2;
+        int ctas = 0;  // 0: as many as fit
+        double ms = 0;  // calibration time of this key (median of the timed runs)
+    };
+    static constexpr int TUNE_MAX_R = 20;
+    TuneCfg tuneTab[2][TUNE_MAX_R + 1];
+    int tunedMaxR = 3;
+
+private:
+    bool tuning = false;  // autotune running: launch times accumulate per key
+    double tuneAccMs[2][TUNE_MAX_R + 1] = {};
+    const TuneCfg &cfg_for(int mode, int r) const
+    {
+        if (mode == MODE_LEAF) return tuneTab[MODE_LEAF][2];
+        return tuneTab[MODE_EXPAND][std::max(3, std::min(r, tunedMaxR))];
+    }
+    int grid_for(int mode, const TuneCfg &c) const
+    {
+        const int occ = gridTile[mode][c.sv];
+        return c.ctas > 0 ? std::min(occ, c.ctas * nsm) : occ;
+    }
+    int max_ctas(int mode, int sv) const { return std::max(1, gridTile[mode][sv] / std::max(1, nsm)); }
+    void fill_tune(int svL, int svE)
+    {
+        for (int r = 0; r <= TUNE_MAX_R; r++) {
+            tuneTab[MODE_LEAF][r] = TuneCfg{svL, TILE_CAP_LOG2, 0, 0};
+            tuneTab[MODE_EXPAND][r] = TuneCfg{svE, TILE_CAP_LOG2, 0, 0};
+        }
+        tunedMaxR = 3;
+    }
+
     void *alloc(u64 bytes)
     {
         const u64 a = (arenaTop + 255) & ~255ULL;
@@ -856,9 +894,9 @@ private:
     }
     u64 arena_free() const { return arenaCap > arenaTop ? arenaCap - arenaTop : 0; }
     bool alloc_level(DeviceLevel &L, u64 n);
-    int scan(const u32 *cnt, u64 n, u64 *&scanOut, u32 *&tileFirst, u64 &total, int &capLog2);
-    int launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst, int capLog2,
-                    u64 itemBase, u64 itemEnd, DeviceLevel *children, unsigned long long *rootCounts);
+    int scan(const u32 *cnt, u64 n, int remaining, u64 *&scanOut, u32 *&tileFirst, u64 &total, int &capLog2);
+    int launch_tile(int mode, int remaining, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst,
+                    int capLog2, u64 itemBase, u64 itemEnd, DeviceLevel *children, unsigned long long *rootCounts);
     int process_level(const DeviceLevel &L, int remaining, unsigned long long *rootCounts);
     int process_level_tt(const DeviceLevel &L, int remaining, unsigned long long *parentAcc,
                          unsigned long long *rootOut);
@@ -879,6 +917,12 @@ public:
     int device_id() const { return device; }
     int leaf_sliders() const { return svLeaf; }
     u64 blockMark = 0;
+    // The transposition table as the server sees it (null table: none configured).
+    struct TTView {
+        ulonglong2 *table;
+        u64 mask, keyMask;
+    };
+    TTView tt_view() const { return TTView{tt, ttMask, ttKeyMask}; }
     int tt_clear();
     void read_tt_stats()
     {
@@ -1075,6 +1119,7 @@ int Engine::init(const perft_config &cfg)
     auto pick = [](int v) { return (v >= 0 && v < SV_COUNT) ? v : SV_KOGGE; };
     svExpand = pick(cfg.sliders_expand);
     svLeaf = pick(cfg.sliders_leaf);
+    fill_tune(svLeaf, svExpand);
     ready = true;
     const bool tuneLeaf = cfg.sliders_leaf == PERFT_SLIDERS_AUTO;
     const bool tuneExpand = cfg.sliders_expand == PERFT_SLIDERS_AUTO;
@@ -1128,7 +1173,9 @@ bool Engine::alloc_level(DeviceLevel &L, u64 n)
     return L.planes && L.cnt && L.root;
 }
 
-int Engine::scan(const u32 *cnt, u64 n, u64 *&scanOut, u32 *&tileFirst, u64 &total, int &capLog2)
+// `remaining`: remaining depth of the level scanned; its items go to the
+// count-only ply when it is 2, to an interior ply otherwise.
+int Engine::scan(const u32 *cnt, u64 n, int remaining, u64 *&scanOut, u32 *&tileFirst, u64 &total, int &capLog2)
 {
     const u64 nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
     const u64 maxTiles = (n * MAX_LEGAL_MOVES) / MAX_TILES_PER_NODE_DIV + 2;
@@ -1142,17 +1189,20 @@ int Engine::scan(const u32 *cnt, u64 n, u64 *&scanOut, u32 *&tileFirst, u64 &tot
     ENG_TRY(cudaMemcpyAsync(hPinned, scanOut + n, 8, cudaMemcpyDeviceToHost, stream));
     ENG_TRY(cudaStreamSynchronize(stream));
     total = hPinned[0];
-    // tile size: as large as possible while every resident CTA still gets tiles
-    capLog2 = TILE_CAP_LOG2;
-    while (capLog2 > TILE_MIN_LOG2 && (total >> capLog2) < 2ull * gridTile[MODE_LEAF][svLeaf]) capLog2--;
+    // tile size: the tuned largest tile for this ply, made smaller while some
+    // resident CTA would get no second tile
+    const int mode = remaining == 2 ? MODE_LEAF : MODE_EXPAND;
+    const TuneCfg &tc = cfg_for(mode, remaining);
+    capLog2 = tc.cap;
+    while (capLog2 > TILE_MIN_LOG2 && (total >> capLog2) < 2ull * grid_for(mode, tc)) capLog2--;
     k_scan_apply<<<(unsigned)nb, SCAN_NT, 0, stream>>>(cnt, n, bsum, scanOut, tileFirst, capLog2);
     stats.other_launches += 3;
     ENG_TRY(cudaGetLastError());
     return PERFT_OK;
 }
 
-int Engine::launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst, int capLog2,
-                        u64 itemBase, u64 itemEnd, DeviceLevel *children,
+int Engine::launch_tile(int mode, int remaining, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst,
+                        int capLog2, u64 itemBase, u64 itemEnd, DeviceLevel *children,
                         unsigned long long *rootCounts)
 {
     TileParams P;
@@ -1177,8 +1227,9 @@ int Engine::launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, 
     P.err = dErr;
 
     const u64 nTiles = (itemEnd - itemBase + (1ull << capLog2) - 1) >> capLog2;
-    const int sv = mode == MODE_LEAF ? svLeaf : svExpand;
-    const int grid = (int)std::min<u64>((u64)gridTile[mode][sv], nTiles);
+    const TuneCfg &tc = cfg_for(mode, remaining);
+    const int sv = tc.sv;
+    const int grid = (int)std::min<u64>((u64)grid_for(mode, tc), nTiles);
     ENG_TRY(cudaMemsetAsync(dCounter, 0, 4, stream));
     ENG_TRY(cudaEventRecord(ev0, stream));
     if (mode == MODE_LEAF) launch_tile_variant<MODE_LEAF>(sv, grid, stream, P);
@@ -1192,6 +1243,7 @@ int Engine::launch_tile(int mode, const DeviceLevel &parents, const u64 *pscan, 
         fprintf(stderr, "perft-trace %s sv=%s parents=%llu items=%llu..%llu grid=%d ms=%.4f\n",
                 mode == MODE_LEAF ? "leaf" : "expand", slider_name(sv), (unsigned long long)parents.n,
                 (unsigned long long)itemBase, (unsigned long long)itemEnd, grid, ms);
+    if (tuning) tuneAccMs[mode][mode == MODE_LEAF ? 2 : std::min(remaining, (int)TUNE_MAX_R)] += ms;
     if (mode == MODE_LEAF) {
         stats.leaf_launches++;
         stats.leaf_items += itemEnd - itemBase;
@@ -1214,14 +1266,14 @@ int Engine::process_level(const DeviceLevel &L, int remaining, unsigned long lon
     u32 *tileFirst = nullptr;
     u64 total = 0;
     int capLog2 = TILE_CAP_LOG2;
-    int rc = scan(L.cnt, L.n, pscan, tileFirst, total, capLog2);
+    int rc = scan(L.cnt, L.n, remaining, pscan, tileFirst, total, capLog2);
     if (rc != PERFT_OK) return rc;
     if (total == 0) {
         arenaTop = mark;
         return PERFT_OK;
     }
     if (remaining == 2) {
-        rc = launch_tile(MODE_LEAF, L, pscan, tileFirst, capLog2, 0, total, nullptr, rootCounts);
+        rc = launch_tile(MODE_LEAF, 2, L, pscan, tileFirst, capLog2, 0, total, nullptr, rootCounts);
         arenaTop = mark;
         return rc;
     }
@@ -1239,7 +1291,7 @@ int Engine::process_level(const DeviceLevel &L, int remaining, unsigned long lon
         const u64 cm = arenaTop;
         DeviceLevel C;
         if (!alloc_level(C, hi - lo)) return PERFT_ERR_OUT_OF_MEMORY;
-        rc = launch_tile(MODE_EXPAND, L, pscan, tileFirst, capLog2, lo, hi, &C, nullptr);
+        rc = launch_tile(MODE_EXPAND, remaining, L, pscan, tileFirst, capLog2, lo, hi, &C, nullptr);
         if (rc != PERFT_OK) return rc;
         rc = process_level(C, remaining - 1, rootCounts);
         if (rc != PERFT_OK) return rc;
@@ -1249,67 +1301,165 @@ int Engine::process_level(const DeviceLevel &L, int remaining, unsigned long lon
     return PERFT_OK;
 }
 
-// Per-ply slider choice: times every variant on a seeded calibration batch
-// (48 playout positions of 10-30 plies at depth 5) and keeps the fastest for
-// the count-only last ply and, separately, for interior plies.
+// Per-depth autotuner.  A seeded calibration batch (32 playouts of 10-30
+// plies at depth 6: interior plies with remaining depth 6..3, then the
+// count-only ply) is run under candidate launch configurations, one warm-up
+// and three timed runs each; every tile launch's CUDA-event time is charged
+// to its (ply kind, remaining depth) key, and each key keeps the median of
+// its three runs.  Coordinate search, every key at once:
+//   1. slider variant (all five), largest tiles, all resident CTAs;
+//   2. largest tile 2^13 / 2^12 / 2^11 items with each key's variant;
+//   3. resident CTAs per SM: all that fit, or one fewer.
+// A candidate replaces a key's current choice only when it is more than 1%
+// faster, so near-ties resolve to the same (earlier) choice on every run.
+// These are the reference's compile-time knobs (switches.h:13-26: block size,
+// memory) chosen per depth on the device at hand.  Results are kept per
+// device for the life of the process (PERFT_RETUNE=1 times again).
 int Engine::autotune(bool leaf, bool expand)
 {
-    constexpr u32 N = 48;
+    struct Cached {
+        TuneCfg tab[2][TUNE_MAX_R + 1];
+        int maxR;
+    };
+    static std::mutex cacheMu;
+    static std::map<std::pair<int, int>, Cached> cache;
+    const std::pair<int, int> key{device, (leaf ? 2 : 0) | (expand ? 1 : 0)};
+    const bool retune = getenv("PERFT_RETUNE") && getenv("PERFT_RETUNE")[0] == '1';
+    auto adopt = [&]() {
+        svLeaf = tuneTab[MODE_LEAF][2].sv;
+        svExpand = tuneTab[MODE_EXPAND][3].sv;
+    };
+    {
+        std::lock_guard<std::mutex> lk(cacheMu);
+        auto it = cache.find(key);
+        if (!retune && it != cache.end()) {
+            for (int m = 0; m < 2; m++) {
+                for (int r = 0; r <= TUNE_MAX_R; r++) {
+                    // a mode that is not tuned keeps the caller's variant
+                    if ((m == MODE_LEAF && !leaf) || (m == MODE_EXPAND && !expand)) continue;
+                    tuneTab[m][r] = it->second.tab[m][r];
+                }
+            }
+            tunedMaxR = it->second.maxR;
+            adopt();
+            return PERFT_OK;
+        }
+    }
+
+    constexpr u32 N = 32;
+    constexpr int CAL_DEPTH = 6;
     std::vector<perft_pos48> pos(N);
     int rc = perft_random_playouts(0xA070707EULL, N, 10, 30, pos.data());
     if (rc != PERFT_OK) return rc;
-    std::vector<uint8_t> depths(N, 5);
+    std::vector<uint8_t> depths(N, CAL_DEPTH);
     const u64 mark = arenaTop;
     u64 *dPos = (u64 *)alloc(48ull * N);
     u64 *dOut = (u64 *)alloc(8ull * N);
     if (!dPos || !dOut) return PERFT_ERR_OUT_OF_MEMORY;
     ENG_TRY(cudaMemcpyAsync(dPos, pos.data(), 48ull * N, cudaMemcpyHostToDevice, stream));
-    const int keepLeaf = svLeaf, keepExpand = svExpand;
     ulonglong2 *keepTT = tt;
     tt = nullptr;  // time the kernels, not table hits
     const bool keepDD = ddEnabled;
     ddEnabled = false;  // the host-driven path times each launch
-    struct RestoreDD {
-        bool &slot, value;
-        ~RestoreDD() { slot = value; }
-    } restoreDD{ddEnabled, keepDD};
     struct Restore {
-        ulonglong2 *&slot, *value;
-        ~Restore() { slot = value; }
-    } restore{tt, keepTT};
-    auto timed = [&](int l, int e, double &leafMs, double &expandMs) -> int {
-        svLeaf = l;
-        svExpand = e;
-        leafMs = expandMs = 1e30;
-        for (int rep = 0; rep < 3; rep++) {
-            const perft_stats before = stats;
-            const int r = run_batch(dPos, depths.data(), N, dOut);
-            if (r != PERFT_OK) return r;
-            if (rep == 0) continue;  // first run warms caches and clocks
-            leafMs = std::min(leafMs, stats.leaf_ms - before.leaf_ms);
-            expandMs = std::min(expandMs, stats.expand_ms - before.expand_ms);
+        Engine &e;
+        ulonglong2 *t;
+        bool dd;
+        u64 mark;
+        ~Restore()
+        {
+            e.tt = t;
+            e.ddEnabled = dd;
+            e.tuning = false;
+            e.arenaTop = mark;
         }
+    } restore{*this, keepTT, keepDD, mark};
+    tunedMaxR = CAL_DEPTH;
+
+    // median over the timed runs of each key's time under the current table
+    double med[2][TUNE_MAX_R + 1];
+    auto measure = [&]() -> int {
+        std::vector<double> reps[2][TUNE_MAX_R + 1];
+        for (int rep = 0; rep < 4; rep++) {
+            memset(tuneAccMs, 0, sizeof tuneAccMs);
+            tuning = true;
+            const perft_stats keep = stats;
+            const int r = run_batch(dPos, depths.data(), N, dOut);
+            stats = keep;  // calibration runs stay out of the statistics
+            tuning = false;
+            if (r != PERFT_OK) return r;
+            if (rep == 0) continue;  // warms caches and clocks
+            for (int m = 0; m < 2; m++)
+                for (int k = 0; k <= TUNE_MAX_R; k++) reps[m][k].push_back(tuneAccMs[m][k]);
+        }
+        for (int m = 0; m < 2; m++)
+            for (int k = 0; k <= TUNE_MAX_R; k++) {
+                std::sort(reps[m][k].begin(), reps[m][k].end());
+                med[m][k] = reps[m][k][reps[m][k].size() / 2];
+            }
         return PERFT_OK;
     };
-    int bestLeaf = keepLeaf, bestExpand = keepExpand;
-    double lm, em, best = 1e30;
-    if (leaf) {
-        for (int v = 0; v < SV_COUNT; v++) {
-            if ((rc = timed(v, keepExpand, lm, em)) != PERFT_OK) return rc;
-            if (lm < best) best = lm, bestLeaf = v;
+    auto keys = [&](auto fn) {  // every tuned (mode, r) key of the calibration
+        if (leaf) fn(MODE_LEAF, 2);
+        if (expand)
+            for (int r = 3; r <= CAL_DEPTH; r++) fn(MODE_EXPAND, r);
+    };
+    double best[2][TUNE_MAX_R + 1];
+    TuneCfg chosen[2][TUNE_MAX_R + 1];
+    auto apply = [&](int m, int r, const TuneCfg &c) {
+        if (m == MODE_LEAF) {
+            for (int k = 0; k <= TUNE_MAX_R; k++) tuneTab[MODE_LEAF][k] = c;
+        } else {
+            tuneTab[MODE_EXPAND][r] = c;
+            if (r == 3)
+                for (int k = 0; k < 3; k++) tuneTab[MODE_EXPAND][k] = c;
+            if (r == CAL_DEPTH)
+                for (int k = CAL_DEPTH + 1; k <= TUNE_MAX_R; k++) tuneTab[MODE_EXPAND][k] = c;
         }
+    };
+    // stage 1: slider variant
+    for (int v = 0; v < SV_COUNT; v++) {
+        keys([&](int m, int r) { apply(m, r, TuneCfg{v, TILE_CAP_LOG2, 0, 0}); });
+        if ((rc = measure()) != PERFT_OK) return rc;
+        keys([&](int m, int r) {
+            if (v == 0 || med[m][r] < 0.99 * best[m][r]) {
+                best[m][r] = med[m][r];
+                chosen[m][r] = TuneCfg{v, TILE_CAP_LOG2, 0, med[m][r]};
+            }
+        });
     }
-    if (expand) {
-        best = 1e30;
-        for (int v = 0; v < SV_COUNT; v++) {
-            if ((rc = timed(bestLeaf, v, lm, em)) != PERFT_OK) return rc;
-            if (em < best) best = em, bestExpand = v;
+    // stage 2: largest tile
+    for (int cap = TILE_CAP_LOG2 - 1; cap >= TILE_CAP_LOG2 - 2 && cap >= TILE_MIN_LOG2; cap--) {
+        keys([&](int m, int r) { apply(m, r, TuneCfg{chosen[m][r].sv, cap, 0, 0}); });
+        if ((rc = measure()) != PERFT_OK) return rc;
+        keys([&](int m, int r) {
+            if (med[m][r] < 0.99 * best[m][r]) {
+                best[m][r] = med[m][r];
+                chosen[m][r] = TuneCfg{chosen[m][r].sv, cap, 0, med[m][r]};
+            }
+        });
+    }
+    // stage 3: one resident CTA per SM fewer
+    keys([&](int m, int r) {
+        const TuneCfg &c = chosen[m][r];
+        apply(m, r, TuneCfg{c.sv, c.cap, std::max(1, max_ctas(m, c.sv) - 1), 0});
+    });
+    if ((rc = measure()) != PERFT_OK) return rc;
+    keys([&](int m, int r) {
+        if (med[m][r] < 0.99 * best[m][r]) {
+            best[m][r] = med[m][r];
+            chosen[m][r] = TuneCfg{chosen[m][r].sv, chosen[m][r].cap, std::max(1, max_ctas(m, chosen[m][r].sv) - 1),
+                                   med[m][r]};
         }
+    });
+    keys([&](int m, int r) { apply(m, r, chosen[m][r]); });
+    adopt();
+    {
+        std::lock_guard<std::mutex> lk(cacheMu);
+        Cached &c = cache[key];
+        memcpy(c.tab, tuneTab, sizeof tuneTab);
+        c.maxR = tunedMaxR;
     }
-    svLeaf = bestLeaf;
-    svExpand = bestExpand;
-    tt = keepTT;
-    arenaTop = mark;
     return PERFT_OK;
 }
 
@@ -1364,13 +1514,13 @@ int Engine::process_level_tt(const DeviceLevel &L, int remaining, unsigned long 
     u32 *tileFirst = nullptr;
     u64 total = 0;
     int capLog2 = TILE_CAP_LOG2;
-    int rc = scan(L.cnt, L.n, pscan, tileFirst, total, capLog2);
+    int rc = scan(L.cnt, L.n, remaining, pscan, tileFirst, total, capLog2);
     if (rc != PERFT_OK) return rc;
     DeviceLevel self = L;
     self.root = nullptr;  // tile sums and child links point at the parent itself
     if (total > 0) {
         if (remaining == 2) {
-            rc = launch_tile(MODE_LEAF, self, pscan, tileFirst, capLog2, 0, total, nullptr, L.acc);
+            rc = launch_tile(MODE_LEAF, 2, self, pscan, tileFirst, capLog2, 0, total, nullptr, L.acc);
             if (rc != PERFT_OK) return rc;
         } else {
             const u64 slack = std::min<u64>(64ull << 20, arenaCap / 16);
@@ -1385,7 +1535,7 @@ int Engine::process_level_tt(const DeviceLevel &L, int remaining, unsigned long 
                 const u64 cm = arenaTop;
                 DeviceLevel C;
                 if (!alloc_level_tt(C, hi - lo)) return PERFT_ERR_OUT_OF_MEMORY;
-                rc = launch_tile(MODE_EXPAND, self, pscan, tileFirst, capLog2, lo, hi, &C, nullptr);
+                rc = launch_tile(MODE_EXPAND, remaining, self, pscan, tileFirst, capLog2, lo, hi, &C, nullptr);
                 if (rc != PERFT_OK) return rc;
                 rc = process_level_tt(C, remaining - 1, L.acc, nullptr);
                 if (rc != PERFT_OK) return rc;
@@ -1513,16 +1663,18 @@ int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, boo
     for (u32 i = 1; i < n; i++)
         if (depths[i] != d) return PERFT_OK;
     if (d < 2 || d > DD_MAX_LEVELS) return PERFT_OK;
-    auto ddSv = [](int v) { return v == SV_KOGGE || v == SV_KOGGE_SPLIT; };
-    if (!ddSv(svLeaf) || !ddSv(svExpand)) return PERFT_OK;
+    // the graph path has the two Kogge-Stone instantiations; another tuned
+    // variant runs there as plain Kogge-Stone (same counts)
+    auto ddSv = [](int v) { return (v == SV_KOGGE || v == SV_KOGGE_SPLIT) ? v : (int)SV_KOGGE; };
+    const int ddL = ddSv(svLeaf), ddE = ddSv(svExpand);
     double est = (double)n * 130.0;
     for (int k = 2; k < d; k++) est *= 40.0;
     if (est > 0.25 * (double)arena_free() && !ddForce) return PERFT_OK;
 
     DDGraph *G = nullptr;
     for (DDGraph &g : ddCache)
-        if (g.depth == d && g.n == n && g.dPos == dPos && g.dOut == dOut && g.top == arenaTop && g.svL == svLeaf &&
-            g.svE == svExpand)
+        if (g.depth == d && g.n == n && g.dPos == dPos && g.dOut == dOut && g.top == arenaTop && g.svL == ddL &&
+            g.svE == ddE)
             G = &g;
     if (!G) {
         if (ddCache.size() >= 16) {
@@ -1541,8 +1693,8 @@ int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, boo
         G->dPos = dPos;
         G->dOut = dOut;
         G->top = arenaTop;
-        G->svL = svLeaf;
-        G->svE = svExpand;
+        G->svL = ddL;
+        G->svE = ddE;
         const int rc = build_dd(*G);
         if (rc != PERFT_OK) {
             drop_dd();
@@ -1711,6 +1863,7 @@ void perft_serve_config_default(perft_serve_config *cfg)
     cfg->memory_bytes = 0;
     cfg->step_items = 1ull << 27;
     cfg->max_in_flight = 4096;
+    cfg->use_tt = 1;
 }
 
 int perft_serve_start(const perft_serve_config *cfg)
@@ -1818,6 +1971,23 @@ int perft_get_stats(perft_stats *out)
     return PERFT_OK;
 }
 
+int perft_get_tuning(perft_tune_entry *out, uint32_t cap, uint32_t *n)
+{
+    if (!n || (!out && cap)) return PERFT_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_engine.mu);
+    if (!g_engine.ready) return PERFT_ERR_NOT_INITIALIZED;
+    uint32_t k = 0;
+    auto put = [&](int leaf, int r) {
+        const Engine::TuneCfg &c = g_engine.tuneTab[leaf ? MODE_LEAF : MODE_EXPAND][r];
+        if (k < cap) out[k] = perft_tune_entry{leaf, r, c.sv, c.cap, c.ctas, c.ms};
+        k++;
+    };
+    put(1, 2);
+    for (int r = 3; r <= g_engine.tunedMaxR; r++) put(0, r);
+    *n = k;
+    return k <= cap ? PERFT_OK : PERFT_ERR_INVALID_ARG;
+}
+
 int perft_tt_clear(void)
 {
     std::lock_guard<std::mutex> lk(g_engine.mu);
@@ -1855,10 +2025,11 @@ int perft_reset_stats(void)
 // calls on a device share it and it keeps the previous call's contents, so
 // each call clears its counters and outputs first.  Two calls whose GPU work
 // overlapped would corrupt each other: this entry point takes a process-wide
-// lock and waits for its work before returning, so its own calls never
-// overlap.  The first call on a device uploads the move-generator tables and
-// looks up the scratch address (cudaGetSymbolAddress) with that device
-// current; make that first call before any stream capture.
+// lock and waits for its stream before returning, on error paths too, so its
+// own calls never overlap.  The first call on a device uploads the
+// move-generator tables and looks up the scratch address
+// (cudaGetSymbolAddress) with that device current; make that first call
+// before any stream capture.
 static __device__ __align__(256) unsigned char g_noallocScratch[PERFT_NOALLOC_SCRATCH_BYTES];
 
 namespace {
@@ -1892,15 +2063,24 @@ __global__ void __launch_bounds__(1024) k_noalloc_group_ids(const uint8_t *__res
     if (threadIdx.x == 0) *count = base;
 }
 
+// Looks up the scratch address with `dev` current, on every call: the lookup
+// allocates nothing and is cheap.  If the address differs from the one cached
+// (first call on the device, or the device's primary context was destroyed and
+// created again, e.g. by cudaDeviceReset), the move tables are uploaded into
+// the current context before the address is trusted.
 int noalloc_setup(int dev)
 {
     NoallocDevice &D = g_noallocDev[dev];
-    if (D.ready) return PERFT_OK;
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noallocScratch) != cudaSuccess || p == nullptr) return PERFT_ERR_CUDA;
+    if (D.ready && D.scratch == (unsigned char *)p) return PERFT_OK;
+    D.ready = false;
     build_tables();
     if (cudaMemcpyToSymbol(d_tables, &h_tables, sizeof(Tables)) != cudaSuccess) return PERFT_ERR_CUDA;
     if (cudaMemcpyToSymbol(d_magic, h_magic, sizeof(h_magic)) != cudaSuccess) return PERFT_ERR_CUDA;
-    void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noallocScratch) != cudaSuccess || p == nullptr) return PERFT_ERR_CUDA;
+    u32 pow2[32];
+    for (int k = 0; k < 32; k++) pow2[k] = 1u << k;
+    if (cudaMemcpyToSymbol(c_pow2, pow2, sizeof pow2) != cudaSuccess) return PERFT_ERR_CUDA;
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return PERFT_ERR_CUDA;
     D.scratch = (unsigned char *)p;
@@ -2032,22 +2212,24 @@ extern "C" int perft_batch_noalloc(const perft_pos48 *d_pos, const uint8_t *dept
     R.counter = (u32 *)R.take(4);
     R.err = (u32 *)R.take(4);
     u32 *dIds = (u32 *)R.take(4ull * n);
-    if (!R.counter || !R.err || !dIds) return PERFT_ERR_OUT_OF_MEMORY;
+    uint8_t *dDepths = (uint8_t *)R.take(n);
+    u32 *dGroupCount = (u32 *)R.take(4);
+    if (!R.counter || !R.err || !dIds || !dDepths || !dGroupCount) return PERFT_ERR_OUT_OF_MEMORY;
+
+    // From the first queued operation on, every return goes through the
+    // stream synchronisation at the end, so the call never returns with work
+    // of its own still queued on the shared scratch (a failed call included).
     unsigned long long *rootCounts = (unsigned long long *)d_out;
-    if (cudaMemsetAsync(R.err, 0, 4, R.st) != cudaSuccess) return PERFT_ERR_CUDA;
-    if (cudaMemsetAsync(rootCounts, 0, 8ull * n, R.st) != cudaSuccess) return PERFT_ERR_CUDA;
+    if (cudaMemsetAsync(R.err, 0, 4, R.st) != cudaSuccess ||
+        cudaMemsetAsync(rootCounts, 0, 8ull * n, R.st) != cudaSuccess ||
+        cudaMemcpyAsync(dDepths, depths, n, cudaMemcpyHostToDevice, R.st) != cudaSuccess)
+        rc = PERFT_ERR_CUDA;
 
     // Group roots by depth without host allocation: the depths go to the
     // scratch and a kernel compacts the ids of one depth group in order.
     u32 perDepth[21] = {0};
     for (u32 i = 0; i < n; i++) perDepth[depths[i]]++;
-    uint8_t *dDepths = (uint8_t *)R.take(n);
-    u32 *dGroupCount = (u32 *)R.take(4);
-    if (!dDepths || !dGroupCount) return PERFT_ERR_OUT_OF_MEMORY;
-    if (cudaMemcpyAsync(dDepths, depths, n, cudaMemcpyHostToDevice, R.st) != cudaSuccess)
-        return PERFT_ERR_CUDA;
-
-    for (int depth = 20; depth >= 0; depth--) {
+    for (int depth = 20; depth >= 0 && rc == PERFT_OK; depth--) {
         const u32 cnt = perDepth[depth];
         if (!cnt) continue;
         const u64 mark = R.top;
@@ -2065,13 +2247,12 @@ extern "C" int perft_batch_noalloc(const perft_pos48 *d_pos, const uint8_t *dept
         }
         if (depth >= 2) rc = R.process(L0, depth, rootCounts);
         R.top = mark;
-        if (rc != PERFT_OK) break;
     }
     u32 e = 0;
-    if (cudaMemcpyAsync(&e, R.err, 4, cudaMemcpyDeviceToHost, R.st) != cudaSuccess ||
-        cudaStreamSynchronize(R.st) != cudaSuccess)
-        return PERFT_ERR_CUDA;
+    const bool readOk = cudaMemcpyAsync(&e, R.err, 4, cudaMemcpyDeviceToHost, R.st) == cudaSuccess;
+    const bool syncOk = cudaStreamSynchronize(R.st) == cudaSuccess;
     if (rc != PERFT_OK) return rc;
+    if (!readOk || !syncOk) return PERFT_ERR_CUDA;
     if (e & DERR_BAD_POSITION) return PERFT_ERR_INVALID_ARG;
     return e ? PERFT_ERR_INTERNAL : PERFT_OK;
 }

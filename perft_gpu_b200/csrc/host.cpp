@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <atomic>
 #include <thread>
+#include <memory>
 #include <mutex>
 #include <random>
 #include <string>
@@ -347,6 +348,41 @@ int frontier_counts(const Frontier &f, u32 depth, u32 shard, u32 n_shards, std::
     return PERFT_OK;
 }
 
+// The frontier of the last sharded deep call.  A rank that takes several
+// shards of one deep search in turn (dynamic dealing: shard j of n as the
+// shared cursor hands them out) builds the frontier once; the enumeration is
+// deterministic, so the cached frontier is the one a rebuild would give.
+// Unsharded calls neither use nor keep it (a frontier can hold gigabytes).
+struct FrontierCache {
+    std::mutex mu;
+    u64 root[6] = {};
+    u32 plies = 0;
+    std::shared_ptr<const Frontier> f;
+} g_frontierCache;
+
+std::shared_ptr<const Frontier> frontier_for(const perft_pos48 *pos, const Board &b, const std::vector<u32> &mv,
+                                             u32 plies, bool sharded)
+{
+    if (!sharded) {
+        std::lock_guard<std::mutex> lk(g_frontierCache.mu);
+        g_frontierCache.f.reset();
+    } else {
+        std::lock_guard<std::mutex> lk(g_frontierCache.mu);
+        if (g_frontierCache.f && g_frontierCache.plies == plies &&
+            memcmp(g_frontierCache.root, pos->bb, sizeof g_frontierCache.root) == 0)
+            return g_frontierCache.f;
+    }
+    auto f = std::make_shared<Frontier>();
+    f->build(b, mv, plies);
+    if (sharded) {
+        std::lock_guard<std::mutex> lk(g_frontierCache.mu);
+        memcpy(g_frontierCache.root, pos->bb, sizeof g_frontierCache.root);
+        g_frontierCache.plies = plies;
+        g_frontierCache.f = f;
+    }
+    return f;
+}
+
 // C-ABI functions return status codes: an exception (host memory
 // exhausted) must not cross the boundary.
 template <class F>
@@ -581,12 +617,13 @@ static int deep_shard_impl(const perft_pos48 *pos, uint32_t depth, uint32_t spli
     build_tables();
     const Board b = from_pos48(pos->bb);
     const std::vector<u32> mv = legal_moves(b);
-    Frontier f;
+    std::shared_ptr<const Frontier> fp;
     try {
-        f.build(b, mv, split_plies);
+        fp = frontier_for(pos, b, mv, split_plies, n_shards > 1);
     } catch (const std::exception &) {
         return PERFT_ERR_OUT_OF_MEMORY;  // host memory or threads exhausted
     }
+    const Frontier &f = *fp;
     std::vector<u64> sub;
     const int rc = frontier_counts(f, depth - 1 - split_plies, shard, n_shards, sub);
     if (rc != PERFT_OK) return rc;

@@ -17,6 +17,18 @@
 // arrive while others run join at the next iteration, and no query waits for
 // another to finish.  A query's count is the same alone or in the mix: it
 // is a sum of exact per-item counts, only the grouping into launches varies.
+//
+// Transposition table: with an engine table and use_tt, every level two plies
+// above the leaves (remaining depth 2) is hashed and probed before its scan,
+// exactly as the engine's own table levels are (k_tt_probe, k_tt_dedup):
+// table hits take the stored count and generate nothing, and identical nodes
+// of the level are searched once.  The level's last ply then sums per node
+// (not per query), and a finish pass stores each searched node, gives every
+// duplicate its owner's count, and adds every node's count to its query.  The
+// table lives in the engine for the life of the process, so it is shared by
+// all queries and keeps its entries across queries.  Nodes two plies above
+// the leaves carry nearly all of the transpositions' savings: the leaf ply
+// below them is ~97% of the work.
 #pragma once
 
 #include <chrono>
@@ -62,10 +74,49 @@ struct ServeQuery {
     u64 result = 0;
 };
 
+// Last step of a table level: owners (and nodes not de-duplicated) store
+// their subtree count, duplicates take their owner's, and every node's count
+// goes to its query with the node's pending mark removed (warp-aggregated per
+// run of equal query slot: the nodes of a level are ordered by query).
+__global__ void __launch_bounds__(256) k_serve_tt_finish(u64 n, const u64 *__restrict__ hash,
+                                                         const u64 *__restrict__ hash2,
+                                                         const unsigned long long *__restrict__ acc,
+                                                         const u32 *__restrict__ alias, const u32 *__restrict__ slot,
+                                                         unsigned long long *counts, unsigned long long *pending,
+                                                         ulonglong2 *tt, u64 ttMask, TTStats *ts)
+{
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    unsigned long long v = 0;
+    u32 key = 0xFFFFFFFFu;
+    bool stored = false;
+    if (i < n) {
+        const u32 a = alias[i];
+        v = acc[i];
+        if (a != ALIAS_HIT && a != ALIAS_NOSLOT && a != (u32)i) {
+            v = acc[a];  // the owner's subtree finished with this level's last launch
+        } else if (a != ALIAS_HIT) {
+            tt[hash[i] & ttMask] = make_ulonglong2(hash2[i] ^ v, v);
+            stored = true;
+        }
+        key = slot[i];
+    }
+    count_stat(&ts->stores, stored);
+    // a count two plies deep is below 218^2 < 2^16, so 32 of them sum in 32 bits
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const unsigned long long sum = __reduce_add_sync(peers, (unsigned)v);
+    if (i < n && lane == __ffs(peers) - 1) {
+        atomicAdd(&counts[key], sum);
+        atomicAdd(&pending[key], (unsigned long long)(-(long long)__popc(peers)));
+    }
+}
+
 struct ServeLevel {
     DeviceLevel L;
     int r = 0;
     bool scanned = false;
+    bool tt = false;  // a table level: per-node sums, finished by k_serve_tt_finish
+    std::vector<std::pair<u64, u64>> ttMem;  // its hashes, sums and aliases
     u64 *pscan = nullptr;
     u32 *tileFirst = nullptr;
     u64 total = 0, next = 0;
@@ -101,6 +152,8 @@ private:
     int complete();
     int scan_level(ServeLevel &S);
     int launch(int mode, ServeLevel &S, u64 lo, u64 hi, DeviceLevel *child);
+    int probe_level(ServeLevel &S);
+    int finish_level(ServeLevel &S);
 
     std::thread worker;
     std::mutex mu;
@@ -125,8 +178,13 @@ private:
     std::vector<ServeLevel *> pools[SERVE_MAX_R + 1];
     u64 budget = 0, reserved = 0, stepItems = 0;
     u32 maxInFlight = 0, inFlight = 0, maxSlotUsed = 0;
-    int gridLeaf = 0, gridExpand = 0;
+    int gridLeaf = 0, gridExpand = 0, gridLeafAcc = 0;
     bool leafSplit = false;
+    // the engine's transposition table, when the server uses it
+    ulonglong2 *tt = nullptr;
+    u64 ttMask = 0, ttKeyMask = ~0ULL;
+    TTStats *dTTStats = nullptr;
+    TTStats *hostTTStats = nullptr;  // pinned
     int idleIterations = 0;
     // statistics
     u64 submitted = 0, completed = 0, iterations = 0, launches = 0, admittedBatches = 0;
@@ -190,16 +248,26 @@ int Server::start(const perft_serve_config &cfg, char *block, u64 bytes, int dev
     counts = (unsigned long long *)take(8ull * SERVE_MAX_SLOTS, fixedMem);
     dCounter = (u32 *)take(256, fixedMem);
     dErr = (u32 *)take(256, fixedMem);
-    if (!posBySlot || !pending || !counts || !dCounter || !dErr) return PERFT_ERR_OUT_OF_MEMORY;
+    dTTStats = (TTStats *)take(256, fixedMem);
+    if (!posBySlot || !pending || !counts || !dCounter || !dErr || !dTTStats) return PERFT_ERR_OUT_OF_MEMORY;
     if (cudaMemsetAsync(dErr, 0, 4, st) != cudaSuccess) return PERFT_ERR_CUDA;
+    if (cudaMemsetAsync(dTTStats, 0, sizeof(TTStats), st) != cudaSuccess) return PERFT_ERR_CUDA;
+    {
+        const Engine::TTView v = g_engine.tt_view();
+        tt = cfg.use_tt ? v.table : nullptr;
+        ttMask = v.mask;
+        ttKeyMask = v.keyMask;
+    }
     budget = std::min<u64>(cfg.memory_bytes ? cfg.memory_bytes : bytes, blockBytes - inUse);
     if (cudaMallocHost(&hostPending, 8ull * SERVE_MAX_SLOTS) != cudaSuccess ||
         cudaMallocHost(&hostCounts, 8ull * SERVE_MAX_SLOTS) != cudaSuccess ||
         cudaMallocHost(&hostTotal, 64) != cudaSuccess ||
         cudaMallocHost(&stagePos, 48ull * SERVE_MAX_SLOTS) != cudaSuccess ||
         cudaMallocHost(&stageSlots, 4ull * SERVE_MAX_SLOTS) != cudaSuccess ||
-        cudaMallocHost(&stageDepths, SERVE_MAX_SLOTS) != cudaSuccess)
+        cudaMallocHost(&stageDepths, SERVE_MAX_SLOTS) != cudaSuccess ||
+        cudaMallocHost(&hostTTStats, sizeof(TTStats)) != cudaSuccess)
         return PERFT_ERR_OUT_OF_MEMORY;
+    memset(hostTTStats, 0, sizeof(TTStats));
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return PERFT_ERR_CUDA;
     cudaFuncSetAttribute(k_tile<MODE_LEAF, SV_KOGGE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -222,6 +290,9 @@ int Server::start(const perft_serve_config &cfg, char *block, u64 bytes, int dev
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_tile<MODE_EXPAND, SV_KOGGE, true>, TILE_NT,
                                                   TILE_DYN_SMEM);
     gridExpand = std::max(1, perSm) * prop.multiProcessorCount;
+    // table levels' last ply: the engine's per-node-sum leaf kernel
+    gridLeafAcc = leafSplit ? occupancy_grid<MODE_LEAF, SV_KOGGE_SPLIT>(prop.multiProcessorCount)
+                            : occupancy_grid<MODE_LEAF, SV_KOGGE>(prop.multiProcessorCount);
     bySlot.assign(SERVE_MAX_SLOTS, nullptr);
     freeSlots.clear();
     for (u32 s = SERVE_MAX_SLOTS; s-- > 0;) freeSlots.push_back(s);
@@ -259,6 +330,7 @@ int Server::stop()
     cudaFreeHost(stagePos);
     cudaFreeHost(stageSlots);
     cudaFreeHost(stageDepths);
+    cudaFreeHost(hostTTStats);
     cudaStreamDestroy(st);
     running = false;
     cvDone.notify_all();
@@ -326,6 +398,10 @@ void Server::get_stats(perft_serve_stats *o)
     o->memory_reserved = reserved;
     o->memory_peak = peakInUse;
     o->last_error = lastError;
+    o->tt_probes = hostTTStats ? hostTTStats->probes : 0;
+    o->tt_hits = hostTTStats ? hostTTStats->hits : 0;
+    o->tt_merged = hostTTStats ? hostTTStats->aliases : 0;
+    o->tt_stores = hostTTStats ? hostTTStats->stores : 0;
 }
 
 int Server::admit()
@@ -407,8 +483,54 @@ int Server::admit()
     return cudaGetLastError() == cudaSuccess ? PERFT_OK : PERFT_ERR_CUDA;
 }
 
+// Hashes and probes a level two plies above the leaves, and de-duplicates
+// its misses; hits and duplicates get no items.  The level keeps the hashes,
+// per-node sums and aliases until k_serve_tt_finish.
+int Server::probe_level(ServeLevel &S)
+{
+    const u64 n = S.L.n;
+    S.L.hash = (u64 *)take(8 * S.L.stride, S.ttMem);
+    S.L.hash2 = (u64 *)take(8 * S.L.stride, S.ttMem);
+    S.L.acc = (unsigned long long *)take(8 * S.L.stride, S.ttMem);
+    S.L.alias = (u32 *)take(4 * S.L.stride, S.ttMem);
+    u64 dsize = 1024;
+    while (dsize < n + n / 4) dsize <<= 1;
+    std::vector<std::pair<u64, u64>> tmp;
+    u64 *dkey = (u64 *)take(8 * dsize, tmp);
+    u32 *downer = (u32 *)take(4 * dsize, tmp);
+    if (!S.L.hash || !S.L.hash2 || !S.L.acc || !S.L.alias || !dkey || !downer) {
+        give_back(tmp);
+        give_back(S.ttMem);  // the next iteration retries from scratch
+        return PERFT_ERR_OUT_OF_MEMORY;
+    }
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    if (cudaMemsetAsync(dkey, 0xFF, 8 * dsize, st) != cudaSuccess ||
+        cudaMemsetAsync(downer, 0xFF, 4 * dsize, st) != cudaSuccess)
+        return PERFT_ERR_CUDA;
+    k_tt_probe<<<nb, 256, 0, st>>>(S.L.planes, S.L.stride, n, 2, true, ttKeyMask, S.L.cnt, S.L.hash, S.L.hash2,
+                                   S.L.acc, S.L.alias, tt, ttMask, dkey, downer, dsize - 1, dTTStats);
+    k_tt_dedup<<<nb, 256, 0, st>>>(n, S.L.cnt, S.L.alias, downer, S.L.hash2, dTTStats);
+    launches += 2;
+    give_back(tmp);  // reused only by later launches on this stream
+    S.tt = true;
+    return cudaGetLastError() == cudaSuccess ? PERFT_OK : PERFT_ERR_CUDA;
+}
+
+int Server::finish_level(ServeLevel &S)
+{
+    const u64 n = S.L.n;
+    k_serve_tt_finish<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, S.L.hash, S.L.hash2, S.L.acc, S.L.alias,
+                                                                    S.L.root, counts, pending, tt, ttMask, dTTStats);
+    launches++;
+    return cudaGetLastError() == cudaSuccess ? PERFT_OK : PERFT_ERR_CUDA;
+}
+
 int Server::scan_level(ServeLevel &S)
 {
+    if (tt && S.r == 2 && !S.tt) {
+        const int rc = probe_level(S);
+        if (rc != PERFT_OK) return rc;
+    }
     const u64 n = S.L.n;
     const u64 nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
     const u64 maxTiles = (n * MAX_LEGAL_MOVES) / MAX_TILES_PER_NODE_DIV + 2;
@@ -423,8 +545,12 @@ int Server::scan_level(ServeLevel &S)
     k_scan_reduce<<<(unsigned)nb, SCAN_NT, 0, st>>>(S.L.cnt, n, bsum);
     k_scan_top<<<1, SCAN_TOP_NT, 0, st>>>(bsum, nb, S.pscan + n);
     k_scan_apply<<<(unsigned)nb, SCAN_NT, 0, st>>>(S.L.cnt, n, bsum, S.pscan, S.tileFirst, TILE_CAP_LOG2);
-    k_serve_zero_parents<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(S.L.cnt, S.L.root, n, pending);
-    launches += 4;
+    launches += 3;
+    // a table level's nodes leave the pending count in its finish pass
+    if (!S.tt) {
+        k_serve_zero_parents<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(S.L.cnt, S.L.root, n, pending);
+        launches++;
+    }
     give_back(tmp);
     if (cudaMemcpyAsync(hostTotal, S.pscan + n, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
@@ -459,7 +585,14 @@ int Server::launch(int mode, ServeLevel &S, u64 lo, u64 hi, DeviceLevel *child)
     P.err = dErr;
     const u64 nTiles = (hi - lo + TILE_CAP - 1) / TILE_CAP;
     if (cudaMemsetAsync(dCounter, 0, 4, st) != cudaSuccess) return PERFT_ERR_CUDA;
-    if (mode == MODE_LEAF && leafSplit)
+    if (mode == MODE_LEAF && S.tt) {
+        // sums per node (the parent's own slot of acc), as the engine's table levels do
+        P.proot = nullptr;
+        P.rootCounts = S.L.acc;
+        P.pending = nullptr;
+        launch_tile_variant<MODE_LEAF>(leafSplit ? SV_KOGGE_SPLIT : SV_KOGGE,
+                                       (int)std::min<u64>(gridLeafAcc, nTiles), st, P);
+    } else if (mode == MODE_LEAF && leafSplit)
         k_tile<MODE_LEAF, SV_KOGGE_SPLIT, true>
             <<<(int)std::min<u64>(gridLeaf, nTiles), TILE_NT, TILE_DYN_SMEM, st>>>(P);
     else if (mode == MODE_LEAF)
@@ -521,7 +654,12 @@ int Server::advance()
                 S->next = hi;
             }
             if (S->next >= S->total) {
+                if (S->tt) {
+                    int rc = finish_level(*S);
+                    if (rc != PERFT_OK) return rc;
+                }
                 give_back(S->mem);
+                give_back(S->ttMem);
                 delete S;
             } else {
                 keep.push_back(S);
@@ -543,6 +681,7 @@ int Server::complete()
     if (!maxSlotUsed) return PERFT_OK;
     if (cudaMemcpyAsync(hostPending, pending, 8ull * maxSlotUsed, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(hostCounts, counts, 8ull * maxSlotUsed, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        (tt && cudaMemcpyAsync(hostTTStats, dTTStats, sizeof(TTStats), cudaMemcpyDeviceToHost, st) != cudaSuccess) ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return PERFT_ERR_CUDA;
     const double t = now_s();

@@ -9,6 +9,8 @@
 // the search is deterministic, so every process builds identical tables.
 #include <string.h>
 
+#include <mutex>
+
 #include "movegen.cuh"
 
 namespace pg {
@@ -103,13 +105,10 @@ u64 find_magic(int sq, u64 mask, const int dirs[4][2], u64 *table, Rng &rng)
     }
 }
 
-bool g_built = false;
+std::once_flag g_builtOnce;
 
-}  // namespace
-
-void build_tables()
+void build_tables_once()
 {
-    if (g_built) return;
     Tables &t = h_tables;
     memset(&t, 0, sizeof(t));
     for (int s = 0; s < 64; s++) {
@@ -151,7 +150,17 @@ void build_tables()
         t.bishopMagic[s] = find_magic(s, mask, BISHOP_DIRS, &h_magic[off], rng);
         off += 1u << popc(mask);
     }
-    g_built = (off == MAGIC_TABLE_ENTRIES);
+}
+
+}  // namespace
+
+// Builds the tables once per process.  Every caller (engine start-up, the
+// allocation-free entry point, the host-side entry points, on any thread)
+// returns only after the tables are complete: std::call_once blocks
+// concurrent callers until the first one has finished filling them.
+void build_tables()
+{
+    std::call_once(g_builtOnce, build_tables_once);
 }
 
 }  // namespace pg

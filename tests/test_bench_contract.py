@@ -54,3 +54,24 @@ def test_reference_arm_other_ranks_exit_quietly():
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
     assert len(lines) == 1 and lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"
+
+
+def test_reference_arm_loads_no_engine_library():
+    """The reference arm reads its workload from the stored numpy file and runs
+    only the reference's host perft: with the engine library made unloadable it
+    still succeeds, and its process never maps libperft_b200."""
+    code = ("import runpy, sys\n"
+            "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0', '--cpu-seconds', '1']\n"
+            "try:\n"
+            "    runpy.run_path('bench.py', run_name='__main__')\n"
+            "except SystemExit as e:\n"
+            "    assert not e.code, e.code\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print('ENGINE_MAPPED' if 'libperft_b200' in maps else 'ENGINE_NOT_MAPPED')\n")
+    env = dict(os.environ, PERFT_B200_LIB=os.path.join(ROOT, "no-such-dir", "libperft_b200.so"))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=ROOT,
+                       env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "ENGINE_NOT_MAPPED" in r.stdout
+    line = json.loads(next(x for x in r.stdout.splitlines() if x.startswith("{")))
+    assert line["cpu_baseline"]["library"].startswith("oracle/")

@@ -80,10 +80,10 @@ def _records_file(engine, path, n=40):
     return pos, occ
 
 
-def test_records_mode_and_resume(engine, tmp_path):
+def test_records_mode_and_resume(engine, oracle, tmp_path):
     path = str(tmp_path / "records.txt")
     pos, occ = _records_file(engine, path)
-    want = engine.perft_batch(pos, np.full(len(pos), 4, dtype=np.uint8))
+    want = oracle.perft_batch_mt(pos, 4)
     assert engine.records(path, 4, batch=16) == len(pos)
     lines = open(path + ".op").read().splitlines()
     src = open(path).read().splitlines()
@@ -123,13 +123,13 @@ def test_cli_perft_lines(golden):
     assert got == {d: counts[str(d)] for d in (3, 4, 5, 6)}
 
 
-def test_cli_records(tmp_path, engine):
+def test_cli_records(tmp_path, engine, oracle):
     path = str(tmp_path / "r.txt")
     pos, occ = _records_file(engine, path, n=10)
     r = subprocess.run([CLI, "--records", path, "3"], capture_output=True, text=True, timeout=300, env=ENV)
     assert r.returncode == 0, r.stderr
     assert "Records done: 10" in r.stdout
-    want = engine.perft_batch(pos, np.full(len(pos), 3, dtype=np.uint8))
+    want = oracle.perft_batch_mt(pos, 3)
     got = [int(line.rsplit(" ", 2)[1]) for line in open(path + ".op").read().splitlines()]
     assert got == [int(x) for x in want]
 

@@ -83,3 +83,56 @@ def test_direct_calls_while_serving(server):
     direct = server.perft_batch(pos, depths)  # the arena engine keeps working beside the server
     got = [server.serve_wait(t, timeout_s=120)[0] for t in tickets]
     assert got == [int(x) for x in direct]
+
+
+@pytest.fixture
+def tt_server(engine):
+    """The server over an engine with a 2^24-entry table."""
+    engine.init(device=0, arena_bytes=6 << 30, tt_log2_entries=24)
+    yield engine
+    engine.serve_stop()
+    engine.init(device=0, arena_bytes=8 << 30)
+
+
+@pytest.mark.parametrize("step_items", [0, 8192], ids=["default", "tiny_steps"])
+def test_served_with_table_equal_alone_and_oracle(tt_server, oracle, step_items):
+    """With the table resident in the server: every query equals its count
+    alone (engine without a table) and the oracle's; identical queries and
+    transpositions are answered from the table or merged."""
+    pos, depths = _queries(tt_server, 200, seed=21, max_depth=6)
+    pos = np.vstack([pos, pos[:40]])  # repeats: answered from the table
+    depths = np.concatenate([depths, depths[:40]])
+    want = oracle.perft_batch_mt(pos, depths)
+    tt_server.serve_start(step_items=step_items)
+    tickets = [tt_server.serve_submit(p, int(d)) for p, d in zip(pos, depths)]
+    got = [tt_server.serve_wait(t, timeout_s=300)[0] for t in tickets]
+    assert got == [int(x) for x in want]
+    st = tt_server.serve_stats()
+    assert st["completed"] == len(pos) and st["last_error"] == 0
+    assert st["tt_probes"] > 0 and st["tt_hits"] > 0 and st["tt_merged"] > 0 and st["tt_stores"] > 0
+    tt_server.serve_stop()
+    # and the same queries without the table in the server
+    tt_server.serve_start(step_items=step_items, use_tt=False)
+    tickets = [tt_server.serve_submit(p, int(d)) for p, d in zip(pos, depths)]
+    assert [tt_server.serve_wait(t, timeout_s=300)[0] for t in tickets] == got
+    assert tt_server.serve_stats()["tt_probes"] == 0
+
+
+def test_served_with_table_shared_slots(engine, oracle, monkeypatch):
+    """A 12-bit slot key: every table and de-duplication slot is shared by
+    many different nodes, so counts stay exact only if the verification key
+    separates them."""
+    monkeypatch.setenv("PERFT_TT_INDEX_KEY_BITS", "12")
+    engine.init(device=0, arena_bytes=6 << 30, tt_log2_entries=20)
+    try:
+        pos, depths = _queries(engine, 120, seed=22, max_depth=5)
+        want = oracle.perft_batch_mt(pos, depths)
+        engine.serve_start()
+        tickets = [engine.serve_submit(p, int(d)) for p, d in zip(pos, depths)]
+        got = [engine.serve_wait(t, timeout_s=300)[0] for t in tickets]
+        assert got == [int(x) for x in want]
+        assert engine.serve_stats()["tt_hits"] > 0
+    finally:
+        engine.serve_stop()
+        monkeypatch.delenv("PERFT_TT_INDEX_KEY_BITS")
+        engine.init(device=0, arena_bytes=8 << 30)

@@ -37,11 +37,13 @@ def test_tt_matches_golden_cold_and_warm(tt_engine, golden):
 
 def test_tt_single_positions_match_no_tt(tt_engine, oracle):
     pos = tt_engine.random_playouts(seed=808, n=40, min_plies=6, max_plies=40)
-    for p in pos[:8]:
-        for d in (2, 3, 4, 5):
-            assert tt_engine.perft(p, d) == oracle.perft(p, d) if d <= 4 else True
+    for d in (2, 3, 4, 5):
+        want = oracle.perft_batch_mt(pos[:8], d)
+        got = [tt_engine.perft(p, d) for p in pos[:8]]
+        assert got == [int(x) for x in want], d
     depths = np.array([5] * 40, dtype=np.uint8)
     got = tt_engine.perft_batch(pos, depths)
+    assert np.array_equal(got, oracle.perft_batch_mt(pos, 5))
     tt_engine.init(device=0, arena_bytes=4 << 30)  # no table
     want = tt_engine.perft_batch(pos, depths)
     assert np.array_equal(got, want)

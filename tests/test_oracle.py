@@ -14,7 +14,9 @@ import pytest
 
 from tests._oracle import P6, ROOT, pos48_from_hex, reference
 
-REF_TREE = "/root/reference"
+# The reference source tree, when this machine has one (the known-position
+# test reads its FEN list at test time).
+REF_TREE = os.environ.get("PERFT_REFERENCE_DIR", "")
 
 
 def test_oracle_matches_golden_counts(oracle, golden):
@@ -71,7 +73,8 @@ def test_oracle_vs_reference_seeded_playouts(oracle):
 
 
 @needs_ref
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF_TREE, "perft.cu")), reason="reference tree absent")
+@pytest.mark.skipif(not (REF_TREE and os.path.exists(os.path.join(REF_TREE, "perft.cu"))),
+                    reason="reference tree absent (set PERFT_REFERENCE_DIR)")
 def test_oracle_vs_reference_known_positions(oracle):
     """The reference keeps its validation positions as FEN strings in
     perft.cu; read them from the reference tree at test time."""
