@@ -403,6 +403,18 @@ def measure_configs(args, pg, device, d_pos, depths, batch_ms_per_step, golden):
     # transposition-table positions at depths 9-10 (2^30 entries), after the
     # depth-8 check without and with the table against the reference
     out["tt_d9_10"] = tt_leg(pg, device, wl, args, golden, timed_steps=1)
+
+    # the 4096-position batch again, through the engine with the 2^30-entry
+    # table (cleared first): effective rate, counts against the reference
+    so = torch.zeros(n, dtype=torch.int64, device="cuda")
+    pg.tt_clear()
+    ms, clk = device_timed(lambda: pg.perft_batch_device(d_pos.data_ptr(), depths, n, so.data_ptr()), 1, device)
+    got = so.cpu().numpy().view(np.uint64)
+    out["batch4096_tt"] = {
+        "workload": BATCH_DESC.format(n=n) + ", with a 2^%d-entry table cleared before the step" % args.tt_log2,
+        "steps": 1, "ms_per_step": ms, "value": float(got.sum()) / (ms / 1e3),
+        "unit": UNIT + " (effective: leaves counted)",
+        "equals_reference": bool(np.array_equal(got, want)) if want is not None else None, "clocks": clk}
     return out
 
 
@@ -624,42 +636,70 @@ def run_tt(args):
 
 
 def run_serve(args):
-    """Serving workload: Poisson arrivals of seeded 0-40-ply positions at
-    depth U[3,7] through the continuous-batching server; p50/p99 latency is
-    submit-to-completion wall time."""
+    """Serving workload: the stored trace of 10,000 seeded 0-40-ply positions
+    at depth U[3,7], submitted with Poisson arrivals at each offered rate of
+    the sweep through the continuous-batching server (table resident in the
+    server when --tt-log2 > 0, cleared between rates).  p50/p99 latency is
+    submit-to-completion time.  Every result is checked against the same
+    query run alone (the batch engine without a table) and against the other
+    rates' results."""
     import perft_gpu_b200 as pg
-    from perft_gpu_b200 import workloads as W
-    pos, depths, arrivals = W.serving_trace(n=args.queries, rate_qps=args.rate, seed=5)
-    pg.init(device=0)
-    pg.serve_start(memory_bytes=int(args.serve_memory_gb * (1 << 30)), step_items=args.serve_step_items)
-    tickets = [None] * len(pos)
-    t_start = time.perf_counter()
-    for i in range(len(pos)):
-        delay = t_start + arrivals[i] - time.perf_counter()
-        if delay > 0:
-            time.sleep(delay)
-        tickets[i] = pg.serve_submit(pos[i], int(depths[i]))
-    lat, counts = np.zeros(len(pos)), np.zeros(len(pos), dtype=np.uint64)
-    for i, t in enumerate(tickets):
-        c, l = pg.serve_wait(t, timeout_s=3600)
-        counts[i], lat[i] = c, l
-    wall = time.perf_counter() - t_start
-    st = pg.serve_stats()
-    pg.serve_stop()
-    # identity: a seeded sample of the queries, recomputed alone
-    sample = np.random.default_rng(1).choice(len(pos), min(256, len(pos)), replace=False)
-    alone = pg.perft_batch(pos[sample], depths[sample])
-    line = {"metric": "serving queries/s with p50/p99 latency", "value": len(pos) / wall, "unit": "queries/s",
-            "n_gpus": 1, "higher_is_better": True, "data": "synthetic", "dtype": "u64",
-            "config": {"workload": "Poisson arrivals, seeded 0-40-ply positions, depth U[3,7]",
-                       "offered_rate_qps": args.rate, "queries": len(pos),
-                       "memory_budget_gb": args.serve_memory_gb or "90% of free arena",
+    import torch
+    torch.cuda.set_device(0)
+    wl = stored_workloads()
+    n = min(args.queries, len(wl["serve_pos"]))
+    pos, depths = wl["serve_pos"][:n], wl["serve_depths"][:n]
+    rates = [float(x) for x in args.rates.split(",")] if args.rates else [args.rate]
+    arena = int(args.arena_gb * (1 << 30))
+
+    pg.init(device=0, arena_bytes=arena)
+    t0 = time.perf_counter()
+    alone = pg.perft_batch(pos, depths)
+    alone_s = time.perf_counter() - t0
+    tt_log2 = args.serve_tt_log2
+    pg.init(device=0, arena_bytes=arena, tt_log2_entries=tt_log2)
+    points = []
+    for rate in rates:
+        arrivals = np.cumsum(np.random.default_rng(5).exponential(1.0 / rate, size=n))
+        if tt_log2:
+            pg.tt_clear()
+        pg.serve_start(memory_bytes=int(args.serve_memory_gb * (1 << 30)), step_items=args.serve_step_items,
+                       use_tt=tt_log2 > 0)
+        tickets = [None] * n
+        with ClockSampler(0) as clk:
+            t_start = time.perf_counter()
+            for i in range(n):
+                delay = t_start + arrivals[i] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                tickets[i] = pg.serve_submit(pos[i], int(depths[i]))
+            lat, counts = np.zeros(n), np.zeros(n, dtype=np.uint64)
+            for i, t in enumerate(tickets):
+                c, l = pg.serve_wait(t, timeout_s=3600)
+                counts[i], lat[i] = c, l
+            wall = time.perf_counter() - t_start
+        st = pg.serve_stats()
+        pg.serve_stop()
+        points.append({"offered_qps": rate, "completed_qps": n / wall, "wall_s": wall,
+                       "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                                     "max": float(lat.max())},
+                       "leaf_nodes_per_s": float(counts.sum()) / wall,
+                       "identical_alone_vs_mix": bool(np.array_equal(alone, counts)),
+                       "server": {k: st[k] for k in ("iterations", "launches", "memory_peak", "tt_probes", "tt_hits",
+                                                     "tt_merged", "tt_stores")},
+                       "clocks": clk.summary()})
+    line = {"metric": "serving queries/s with p50/p99 latency", "unit": "queries/s", "n_gpus": 1,
+            "higher_is_better": True, "data": "synthetic", "dtype": "u64",
+            "value": max(p["completed_qps"] for p in points),
+            "config": {"workload": "Poisson arrivals of the stored 0-40-ply positions, depth U[3,7]",
+                       "queries": n, "memory_budget_gb": args.serve_memory_gb,
+                       "transposition_table": f"2^{tt_log2} x 16 B, resident in the server, cleared between rates"
+                       if tt_log2 else "none",
                        "step_items": args.serve_step_items or "server default"},
-            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                          "max": float(lat.max())},
-            "leaf_nodes_per_s": float(counts.sum()) / wall,
-            "identical_alone_vs_mix": bool(np.array_equal(alone, counts[sample])),
-            "server": {k: st[k] for k in ("iterations", "launches", "memory_peak")}}
+            "alone": {"engine": "perft_batch without a table", "seconds": alone_s,
+                      "leaves": int(alone.sum())},
+            "sweep": points,
+            "timing": "host wall clock (submit to completion per query; whole trace for q/s)"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -686,7 +726,10 @@ def main():
     ap.add_argument("--parity-depth", type=int, default=8,
                     help="tt workload: depth of the table vs no-table equality check")
     ap.add_argument("--rate", type=float, default=1000.0, help="serve workload: offered queries/s")
-    ap.add_argument("--queries", type=int, default=2000, help="serve workload: trace length")
+    ap.add_argument("--rates", default="", help="serve workload: comma-separated offered rates to sweep")
+    ap.add_argument("--queries", type=int, default=10000, help="serve workload: trace length")
+    ap.add_argument("--serve-tt-log2", type=int, default=30,
+                    help="serve workload: table entries (log2) resident in the server; 0 = no table")
     ap.add_argument("--serve-memory-gb", type=float, default=120.0, help="serve workload: admission budget")
     ap.add_argument("--serve-step-items", type=int, default=0,
                     help="serve workload: items per level per scheduler step (0 = server default)")

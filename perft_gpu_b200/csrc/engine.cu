@@ -11,8 +11,9 @@
 // Design (B200-first):
 //   * Boards are side-relative (movegen.cuh), so no kernel branches on the
 //     side to move.
-//   * A level is a structure-of-arrays buffer in HBM: six u64 planes plus
-//     the move count and root id of each node.  Every node of a level has
+//   * A level is a structure-of-arrays buffer in HBM: the boards as three
+//     arrays of 16-byte plane pairs (128-bit loads and stores), plus the move
+//     count and root id of each node.  Every node of a level has
 //     the same remaining depth (roots are grouped by depth).
 //   * One exclusive scan of the move counts turns a level into a flat list
 //     of (parent, move) items.  Items are cut into fixed tiles of TILE_CAP;
@@ -89,6 +90,27 @@ enum { MODE_EXPAND = 0, MODE_LEAF = 1 };
 // share of the tile index (4 B per TILE_CAP items, up to 218 items a node)
 // and of the scan's block sums, rounded up.
 constexpr u64 NODE_BYTES = 6 * 8 + 4 + 4 + 8 + 1;  // (tile index sized for the smallest tile: < 1 B/node)
+
+// ------------------------------------------------------- level node boards
+// A level's boards in HBM are a structure of arrays of plane pairs: pair j of
+// node g (planes 2j and 2j+1: mine/pawns, knights/bq, rq/kings) is one
+// 16-byte vector at pp[j * stride + g].  A node is written with three 128-bit
+// stores and read with three 128-bit loads, and a warp's 32 consecutive nodes
+// touch 512 contiguous bytes per pair.  48 bytes per node, as six u64 planes.
+__device__ __forceinline__ void level_put(u64 *planes, u64 stride, u64 g, const Board &b)
+{
+    ulonglong2 *pp = reinterpret_cast<ulonglong2 *>(planes);
+    pp[g] = make_ulonglong2(b.mine, b.pawns);
+    pp[stride + g] = make_ulonglong2(b.knights, b.bq);
+    pp[2 * stride + g] = make_ulonglong2(b.rq, b.kings);
+}
+
+__device__ __forceinline__ Board level_get(const u64 *planes, u64 stride, u64 g)
+{
+    const ulonglong2 *pp = reinterpret_cast<const ulonglong2 *>(planes);
+    const ulonglong2 a = pp[g], c = pp[stride + g], d = pp[2 * stride + g];
+    return Board{a.x, a.y, c.x, c.y, d.x, d.y};
+}
 
 // --------------------------------------------------------- block helpers
 template <int NT>
@@ -225,12 +247,7 @@ __global__ void k_init_roots(const u64 *__restrict__ pos48, const u32 *__restric
     } else {
         c = count_moves<SV_KOGGE>(b);
     }
-    planes[0 * stride + i] = b.mine;
-    planes[1 * stride + i] = b.pawns;
-    planes[2 * stride + i] = b.knights;
-    planes[3 * stride + i] = b.bq;
-    planes[4 * stride + i] = b.rq;
-    planes[5 * stride + i] = b.kings;
+    level_put(planes, stride, i, b);
     cnt[i] = c;
     root[i] = id;
     if (depth == 0) rootCounts[id] = 1ull;
@@ -484,8 +501,13 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
             if (valid) {
                 qEnd = P.pscan[q + 1];
                 if (TRACK) sqEnd[tid] = qEnd;
-#pragma unroll
-                for (int k = 0; k < 6; k++) sb[k][tid] = P.ppl[k * P.pstride + q];
+                const Board pb = level_get(P.ppl, P.pstride, q);
+                sb[0][tid] = pb.mine;
+                sb[1][tid] = pb.pawns;
+                sb[2][tid] = pb.knights;
+                sb[3][tid] = pb.bq;
+                sb[4][tid] = pb.rq;
+                sb[5][tid] = pb.kings;
                 sroot[tid] = P.proot ? P.proot[q] : (u32)q;  // no root array: account to the parent itself
             }
             const u64 sBeg = max(P.pscan[p], iBeg);
@@ -543,12 +565,7 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
                         cnt = count_moves<SV>(ch);
                         if (MODE == MODE_EXPAND) {
                             const u64 g = sBeg + (u64)j - P.itemBase;
-                            P.cpl[0 * P.cstride + g] = ch.mine;
-                            P.cpl[1 * P.cstride + g] = ch.pawns;
-                            P.cpl[2 * P.cstride + g] = ch.knights;
-                            P.cpl[3 * P.cstride + g] = ch.bq;
-                            P.cpl[4 * P.cstride + g] = ch.rq;
-                            P.cpl[5 * P.cstride + g] = ch.kings;
+                            level_put(P.cpl, P.cstride, g, ch);
                             P.ccnt[g] = cnt;
                             P.croot[g] = sroot[pl];
                         }
@@ -675,8 +692,7 @@ __global__ void __launch_bounds__(256) k_tt_probe(const u64 *__restrict__ planes
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     bool hit = false;
     if (i < n) {
-        const Board b{planes[i], planes[stride + i], planes[2 * stride + i], planes[3 * stride + i],
-                      planes[4 * stride + i], planes[5 * stride + i]};
+        const Board b = level_get(planes, stride, i);
         ulonglong2 z = zobrist_rel(b);
         zx(z, ZOB_KEYS + remaining);
         const u64 h = z.x & keyMask;  // slot key (table index, de-duplication set)
