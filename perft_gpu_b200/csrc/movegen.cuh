@@ -61,14 +61,6 @@
 #ifndef PG_GEN_MAGIC
 #define PG_GEN_MAGIC 1
 #endif
-// PG_COUNT_MAGIC_ATT: where the fused count's opponent slider attack map
-// comes from.  0 = the Kogge-Stone fills shared with this side's move fills;
-// bit 0 / bit 1 set = rook-type / bishop-type attacks by one magic lookup per
-// opponent slider (own king transparent), the fills of that type then only
-// count this side's moves.
-#ifndef PG_COUNT_MAGIC_ATT
-#define PG_COUNT_MAGIC_ATT 0
-#endif
 // PG_GEN_MAGIC_ATTACKS 1: generation also builds the opponent's attack map
 // from magic lookups, one per opponent slider.
 #ifndef PG_GEN_MAGIC_ATTACKS
@@ -722,32 +714,28 @@ PG_HD u32 count_moves_fused(const Board &b)
             x &= x - 1;
         }
     } else {
-        // opponent fill generators: none when the attack map comes from lookups
-        const u64 eR = (PG_COUNT_MAGIC_ATT & 1) ? 0 : tR, eB = (PG_COUNT_MAGIC_ATT & 2) ? 0 : tB;
-        if (PG_COUNT_MAGIC_ATT & 1) for_each_bit(tR, [&](int s) { attacked |= magic_rook(s, occ ^ myK); });
-        if (PG_COUNT_MAGIC_ATT & 2) for_each_bit(tB, [&](int s) { attacked |= magic_bishop(s, occ ^ myK); });
 #if PG_KS_LINE
-        ks_line<8, M>(eR, R, empty, ~0ULL, ~0ULL, targets, attacked, n);
+        ks_line<8, M>(tR, R, empty, ~0ULL, ~0ULL, targets, attacked, n);
 #else
-        ks_pair<8, true, M>(eR, R, empty, ~0ULL, targets, attacked, n);
-        ks_pair<8, false, M>(eR, R, empty, ~0ULL, targets, attacked, n);
+        ks_pair<8, true, M>(tR, R, empty, ~0ULL, targets, attacked, n);
+        ks_pair<8, false, M>(tR, R, empty, ~0ULL, targets, attacked, n);
 #endif
         if (PG_RANK_SUB) {
-            rank_pair<false>(eR, R, occ | FILEA, targets, attacked, n);
-            rank_pair<true>(eR, R, brev64(occ) | FILEA, targets, attacked, n);
+            rank_pair<false>(tR, R, occ | FILEA, targets, attacked, n);
+            rank_pair<true>(tR, R, brev64(occ) | FILEA, targets, attacked, n);
         } else {
-            ks_pair<1, true, M>(eR, R, empty, ~FILEA, targets, attacked, n);
-            ks_pair<1, false, M>(eR, R, empty, ~FILEH, targets, attacked, n);
+            ks_pair<1, true, M>(tR, R, empty, ~FILEA, targets, attacked, n);
+            ks_pair<1, false, M>(tR, R, empty, ~FILEH, targets, attacked, n);
         }
 #if PG_KS_LINE
         const u64 inner = empty & ~(FILEA | FILEH);
-        ks_line<9, M>(eB, B, inner, ~FILEA, ~FILEH, targets, attacked, n);  // north-east, south-west
-        ks_line<7, M>(eB, B, inner, ~FILEH, ~FILEA, targets, attacked, n);  // north-west, south-east
+        ks_line<9, M>(tB, B, inner, ~FILEA, ~FILEH, targets, attacked, n);  // north-east, south-west
+        ks_line<7, M>(tB, B, inner, ~FILEH, ~FILEA, targets, attacked, n);  // north-west, south-east
 #else
-        ks_pair<9, true, M>(eB, B, empty, ~FILEA, targets, attacked, n);
-        ks_pair<7, true, M>(eB, B, empty, ~FILEH, targets, attacked, n);
-        ks_pair<7, false, M>(eB, B, empty, ~FILEA, targets, attacked, n);
-        ks_pair<9, false, M>(eB, B, empty, ~FILEH, targets, attacked, n);
+        ks_pair<9, true, M>(tB, B, empty, ~FILEA, targets, attacked, n);
+        ks_pair<7, true, M>(tB, B, empty, ~FILEH, targets, attacked, n);
+        ks_pair<7, false, M>(tB, B, empty, ~FILEA, targets, attacked, n);
+        ks_pair<9, false, M>(tB, B, empty, ~FILEH, targets, attacked, n);
 #endif
     }
     attacked |= pawn_att_down(tP) | knight_set_att(tN) | PG_TAB(king[ctz(b.kings & theirs)]);
