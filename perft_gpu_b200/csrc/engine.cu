@@ -268,7 +268,8 @@ struct LevelDesc {
     u64 stride;
     u32 *cnt;
     u32 *root;
-    u64 n;
+    u64 n;        // nodes: the previous ply's children, then the roots joining here
+    u64 nChild;   // children written by the previous ply's tile kernel
     u64 *pscan;
     u32 *tileFirst;
     u64 *bsum;
@@ -284,6 +285,10 @@ struct DevPlan {
     u32 overflow;
     u32 tileTarget;  // smallest tile count a level should have (2 x resident CTAs)
     LevelDesc lv[DD_MAX_LEVELS];
+    // roots that join level k (their depth is the level's remaining depth)
+    u32 joinN[DD_MAX_LEVELS];
+    const u32 *joinIds[DD_MAX_LEVELS];
+    int capMax[DD_MAX_LEVELS];  // largest tile (log2 items) for the items of level k
 };
 
 __device__ __forceinline__ void *dd_take(DevPlan *plan, u64 bytes)
@@ -334,13 +339,14 @@ __global__ void __launch_bounds__(SCAN_TOP_NT) k_dd_scan_top(DevPlan *plan, int 
     if (threadIdx.x != 0) return;
     if (n) L.pscan[n] = total;
     L.total = plan->overflow ? 0 : total;
-    int cap = TILE_CAP_LOG2;
+    int cap = plan->capMax[lv] ? plan->capMax[lv] : TILE_CAP_LOG2;
     while (cap > TILE_MIN_LOG2 && (total >> cap) < plan->tileTarget) cap--;
     L.capLog2 = cap;
     if (last) return;
     LevelDesc &C = plan->lv[lv + 1];
-    const u64 m = L.total;
+    const u64 m = L.total + plan->joinN[lv + 1];
     C.n = m;
+    C.nChild = L.total;
     C.stride = (m + 31) & ~31ULL;
     C.total = 0;
     C.planes = (u64 *)dd_take(plan, 48 * C.stride);
@@ -388,6 +394,29 @@ __global__ void __launch_bounds__(SCAN_NT) k_dd_scan_apply(DevPlan *plan, int lv
         }
         __syncthreads();
     }
+}
+
+// Roots joining level lv of a device-driven run: written behind the
+// children, from the position array (as k_init_roots does).  Nothing is
+// written into a level that overflowed the plan.
+__global__ void k_dd_join(DevPlan *plan, int lv, const u64 *__restrict__ pos48, u32 *err)
+{
+    const LevelDesc &C = plan->lv[lv];
+    const u32 nj = plan->joinN[lv];
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nj || C.n == 0 || plan->overflow) return;
+    const u32 id = plan->joinIds[lv][i];
+    u64 p[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) p[k] = pos48[6 * (u64)id + k];
+    u32 c = 0;
+    const Board b = from_pos48(p);
+    if (validate_pos48(p) != 0) atomicOr(err, DERR_BAD_POSITION);
+    else c = count_moves<SV_KOGGE>(b);
+    const u64 g = C.nChild + i;
+    level_put(C.planes, C.stride, g, b);
+    C.cnt[g] = c;
+    C.root[g] = id;
 }
 
 // ------------------------------------------------------------ tile kernel
@@ -913,7 +942,17 @@ private:
     int scan(const u32 *cnt, u64 n, int remaining, u64 *&scanOut, u32 *&tileFirst, u64 &total, int &capLog2);
     int launch_tile(int mode, int remaining, const DeviceLevel &parents, const u64 *pscan, const u32 *tileFirst,
                     int capLog2, u64 itemBase, u64 itemEnd, DeviceLevel *children, unsigned long long *rootCounts);
-    int process_level(const DeviceLevel &L, int remaining, unsigned long long *rootCounts);
+    // Roots that join the search at a given remaining depth: their ids (device
+    // array) and count, indexed by depth.  A root of depth d enters the level
+    // whose nodes have d plies left, behind that level's children.
+    struct Joiners {
+        const u64 *dPos = nullptr;
+        const u32 *ids[21] = {};
+        u32 n[21] = {};
+    };
+    int process_level(const DeviceLevel &L, int remaining, unsigned long long *rootCounts,
+                      const Joiners *join = nullptr);
+    int init_joiners(const Joiners &J, int depth, DeviceLevel &C, u64 at, unsigned long long *rootCounts);
     int process_level_tt(const DeviceLevel &L, int remaining, unsigned long long *parentAcc,
                          unsigned long long *rootOut);
     bool alloc_level_tt(DeviceLevel &L, u64 n);
@@ -968,12 +1007,15 @@ private:
 
     // device-driven runs captured as CUDA graphs (small single-depth batches)
     struct DDGraph {
-        int depth = 0;
+        int depth = 0;                // deepest root
+        std::vector<uint8_t> depths;  // every root's depth (the graph's plan depends on the mix)
         u32 n = 0;
         const u64 *dPos = nullptr;
         u64 *dOut = nullptr;
         u64 top = 0;
         int svL = 0, svE = 0;
+        bool overflowed = false;  // the plan did not fit: later calls go host-driven at once
+        cudaEvent_t evLeaf0 = nullptr, evLeaf1 = nullptr;  // recorded around the count-only ply
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         DevPlan *hTemplate = nullptr;  // pinned
@@ -1274,42 +1316,68 @@ int Engine::launch_tile(int mode, int remaining, const DeviceLevel &parents, con
 }
 
 // L holds the nodes of one level, all with `remaining` plies left (>= 2).
-int Engine::process_level(const DeviceLevel &L, int remaining, unsigned long long *rootCounts)
+// Writes the roots that join at remaining depth `depth` into C from index `at`.
+int Engine::init_joiners(const Joiners &J, int depth, DeviceLevel &C, u64 at, unsigned long long *rootCounts)
 {
-    if (L.n == 0) return PERFT_OK;
+    const u32 nj = J.n[depth];
+    if (!nj) return PERFT_OK;
+    k_init_roots<<<(nj + 127) / 128, 128, 0, stream>>>(J.dPos, J.ids[depth], nj, C.planes + 2 * at, C.stride,
+                                                        C.cnt + at, C.root + at, depth, rootCounts, dErr);
+    stats.other_launches++;
+    return check(cudaGetLastError(), "k_init_roots");
+}
+
+// L holds the nodes of one level, all with `remaining` plies left (>= 2).
+// With `join`, the roots of depth remaining - 1 are appended to the children
+// (to the last chunk when the children are chunked), so every depth group of
+// a batch shares one launch per ply: the deepest roots start the search and
+// shallower ones join the level whose remaining depth equals theirs.
+int Engine::process_level(const DeviceLevel &L, int remaining, unsigned long long *rootCounts, const Joiners *join)
+{
+    const u32 nJoin = (join && remaining - 1 >= 2) ? join->n[remaining - 1] : 0;
+    if (L.n == 0 && nJoin == 0) return PERFT_OK;
     const u64 mark = arenaTop;
     u64 *pscan = nullptr;
     u32 *tileFirst = nullptr;
     u64 total = 0;
     int capLog2 = TILE_CAP_LOG2;
-    int rc = scan(L.cnt, L.n, remaining, pscan, tileFirst, total, capLog2);
+    int rc = L.n ? scan(L.cnt, L.n, remaining, pscan, tileFirst, total, capLog2) : PERFT_OK;
     if (rc != PERFT_OK) return rc;
-    if (total == 0) {
-        arenaTop = mark;
-        return PERFT_OK;
-    }
     if (remaining == 2) {
-        rc = launch_tile(MODE_LEAF, 2, L, pscan, tileFirst, capLog2, 0, total, nullptr, rootCounts);
+        if (total) rc = launch_tile(MODE_LEAF, 2, L, pscan, tileFirst, capLog2, 0, total, nullptr, rootCounts);
         arenaTop = mark;
         return rc;
+    }
+    if (total == 0 && nJoin == 0) {
+        arenaTop = mark;
+        return PERFT_OK;
     }
     // interior ply: children fit whole, or in tile-aligned chunks
     const u64 slack = std::min<u64>(64ull << 20, arenaCap / 16);
     const u64 freeB = arena_free() > slack ? arena_free() - slack : 0;
     u64 budgetNodes = freeB / NODE_BYTES;
     if (remaining > 3) budgetNodes /= 2;  // leave room for the plies below
+    budgetNodes = budgetNodes > nJoin ? budgetNodes - nJoin : 0;
     // whole level when it fits; otherwise tile-aligned chunks
     u64 chunk = total <= budgetNodes ? total : (budgetNodes & ~(u64)(TILE_CAP - 1));
-    if (chunk == 0) return PERFT_ERR_OUT_OF_MEMORY;
+    if (chunk == 0 && total) return PERFT_ERR_OUT_OF_MEMORY;
     if (chunk < total) stats.chunked_levels++;
-    for (u64 lo = 0; lo < total; lo += chunk) {
-        const u64 hi = std::min(total, lo + chunk);
+    const u64 nChunks = total ? (total + chunk - 1) / chunk : 1;
+    for (u64 k = 0; k < nChunks; k++) {
+        const u64 lo = k * chunk, hi = std::min(total, lo + chunk);
+        const bool last = k + 1 == nChunks;
         const u64 cm = arenaTop;
         DeviceLevel C;
-        if (!alloc_level(C, hi - lo)) return PERFT_ERR_OUT_OF_MEMORY;
-        rc = launch_tile(MODE_EXPAND, remaining, L, pscan, tileFirst, capLog2, lo, hi, &C, nullptr);
-        if (rc != PERFT_OK) return rc;
-        rc = process_level(C, remaining - 1, rootCounts);
+        if (!alloc_level(C, (hi - lo) + (last ? nJoin : 0))) return PERFT_ERR_OUT_OF_MEMORY;
+        if (hi > lo) {
+            rc = launch_tile(MODE_EXPAND, remaining, L, pscan, tileFirst, capLog2, lo, hi, &C, nullptr);
+            if (rc != PERFT_OK) return rc;
+        }
+        if (last && nJoin) {
+            rc = init_joiners(*join, remaining - 1, C, hi - lo, rootCounts);
+            if (rc != PERFT_OK) return rc;
+        }
+        rc = process_level(C, remaining - 1, rootCounts, join);
         if (rc != PERFT_OK) return rc;
         arenaTop = cm;
     }
@@ -1580,16 +1648,33 @@ void Engine::drop_dd()
         cudaFreeHost(G.hTemplate);
         cudaFreeHost(G.hIds);
         cudaFreeHost(G.hFlags);
+        if (G.evLeaf0) cudaEventDestroy(G.evLeaf0);
+        if (G.evLeaf1) cudaEventDestroy(G.evLeaf1);
     }
     ddCache.clear();
 }
 
-// Captures one device-driven perft of G.n roots at G.depth.  Every buffer the
-// graph reads is re-initialised inside it (plan, root ids, outputs), so the
-// region above the arena top may be reused by other calls between replays.
+// Captures one device-driven perft of G.n roots of any depth mix.  The
+// deepest roots form level 0; a root of depth d joins level G.depth - d
+// (behind that level's children), so every ply of the whole batch is one
+// scan and one tile launch.  Roots of depth 0 and 1 are answered by
+// k_init_roots.  Every buffer the graph reads is re-initialised inside it
+// (plan, root ids, outputs), so the region above the arena top may be reused
+// by other calls between replays.
 int Engine::build_dd(DDGraph &G)
 {
     const u64 n = G.n;
+    const int d = G.depth;
+    std::vector<u32> order;
+    order.reserve(n);
+    u32 nAt[DD_MAX_LEVELS + 2] = {};
+    u64 offAt[DD_MAX_LEVELS + 2] = {};
+    for (int dd = d; dd >= 0; dd--) {
+        offAt[dd] = order.size();
+        for (u32 i = 0; i < n; i++)
+            if (G.depths[i] == dd) order.push_back(i);
+        nAt[dd] = (u32)(order.size() - offAt[dd]);
+    }
     const u64 off0 = (arenaTop + 255) & ~255ULL;
     char *base = arena + off0;
     const u64 cap = arenaCap - off0;
@@ -1601,36 +1686,67 @@ int Engine::build_dd(DDGraph &G)
     };
     DevPlan *dPlan = (DevPlan *)place(sizeof(DevPlan));
     u32 *dIds = (u32 *)place(4 * n);
+    const u64 n0 = nAt[d];
     LevelDesc L0{};
-    L0.n = n;
-    L0.stride = (n + 31) & ~31ULL;
+    L0.n = n0;
+    L0.nChild = 0;
+    L0.stride = (n0 + 31) & ~31ULL;
     L0.planes = (u64 *)place(48 * L0.stride);
     L0.cnt = (u32 *)place(4 * L0.stride);
     L0.root = (u32 *)place(4 * L0.stride);
-    L0.pscan = (u64 *)place(8 * (n + 1));
-    L0.tileFirst = (u32 *)place(4 * ((n * MAX_LEGAL_MOVES) / MAX_TILES_PER_NODE_DIV + 2));
-    L0.bsum = (u64 *)place(8 * ((n + SCAN_CHUNK - 1) / SCAN_CHUNK + 1));
+    L0.pscan = (u64 *)place(8 * (n0 + 1));
+    L0.tileFirst = (u32 *)place(4 * ((n0 * MAX_LEGAL_MOVES) / MAX_TILES_PER_NODE_DIV + 2));
+    L0.bsum = (u64 *)place(8 * ((n0 + SCAN_CHUNK - 1) / SCAN_CHUNK + 1));
+    // scratch level for the roots of depth 0 and 1 (counts only)
+    const u64 nShallow = std::max<u64>(nAt[0], nAt[1]);
+    const u64 sStride = (nShallow + 31) & ~31ULL;
+    u64 *sPlanes = (u64 *)place(48 * std::max<u64>(sStride, 32));
+    u32 *sCnt = (u32 *)place(4 * std::max<u64>(sStride, 32));
+    u32 *sRoot = (u32 *)place(4 * std::max<u64>(sStride, 32));
     if (bump > cap) return PERFT_ERR_OUT_OF_MEMORY;
 
     ENG_TRY(cudaMallocHost(&G.hTemplate, sizeof(DevPlan)));
     ENG_TRY(cudaMallocHost(&G.hIds, 4 * n));
     ENG_TRY(cudaMallocHost(&G.hFlags, 64));
+    ENG_TRY(cudaEventCreate(&G.evLeaf0));
+    ENG_TRY(cudaEventCreate(&G.evLeaf1));
     memset(G.hTemplate, 0, sizeof(DevPlan));
     G.hTemplate->base = base;
     G.hTemplate->cap = cap;
     G.hTemplate->bump = bump;
     G.hTemplate->tileTarget = 2 * gridTile[MODE_LEAF][G.svL];
     G.hTemplate->lv[0] = L0;
-    for (u32 i = 0; i < n; i++) G.hIds[i] = i;
+    for (int dd = 2; dd < d; dd++) {
+        G.hTemplate->joinN[d - dd] = nAt[dd];
+        G.hTemplate->joinIds[d - dd] = dIds + offAt[dd];
+    }
+    // per ply: the tuned variant (one of the two graph instantiations) and largest tile
+    auto ddSv = [](int v) { return (v == SV_KOGGE || v == SV_KOGGE_SPLIT) ? v : (int)SV_KOGGE; };
+    int lvSv[DD_MAX_LEVELS] = {}, lvGrid[DD_MAX_LEVELS] = {};
+    for (int lv = 0; lv <= d - 2; lv++) {
+        const int r = d - lv, mode = r == 2 ? MODE_LEAF : MODE_EXPAND;
+        TuneCfg c = cfg_for(mode, r);
+        c.sv = ddSv(c.sv);
+        lvSv[lv] = c.sv;
+        lvGrid[lv] = grid_for(mode, c);
+        G.hTemplate->capMax[lv] = c.cap;
+    }
+    memcpy(G.hIds, order.data(), 4 * n);
 
-    const int d = G.depth;
     ENG_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     cudaMemcpyAsync(dPlan, G.hTemplate, sizeof(DevPlan), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(dIds, G.hIds, 4 * n, cudaMemcpyHostToDevice, stream);
     cudaMemsetAsync(G.dOut, 0, 8 * n, stream);
     cudaMemsetAsync(dErr, 0, 4, stream);
-    k_init_roots<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(G.dPos, dIds, (u32)n, L0.planes, L0.stride, L0.cnt,
-                                                                  L0.root, d, (unsigned long long *)G.dOut, dErr);
+    for (int dd = 0; dd <= 1; dd++)
+        if (nAt[dd])
+            k_init_roots<<<(nAt[dd] + 127) / 128, 128, 0, stream>>>(G.dPos, dIds + offAt[dd], nAt[dd], sPlanes,
+                                                                   sStride, sCnt, sRoot, dd,
+                                                                   (unsigned long long *)G.dOut, dErr);
+    if (d >= 2)
+        k_init_roots<<<(unsigned)((n0 + 127) / 128), 128, 0, stream>>>(G.dPos, dIds + offAt[d], (u32)n0,
+                                                                      L0.planes, L0.stride, L0.cnt, L0.root, d,
+                                                                      (unsigned long long *)G.dOut, dErr);
     for (int lv = 0; lv <= d - 2; lv++) {
         const int last = lv == d - 2;
         k_dd_scan_reduce<<<ddGridScan, SCAN_NT, 0, stream>>>(dPlan, lv);
@@ -1644,19 +1760,26 @@ int Engine::build_dd(DDGraph &G)
         P.tileCounter = dCounter;
         P.rootCounts = (unsigned long long *)G.dOut;
         P.err = dErr;
-        const int sv = last ? G.svL : G.svE;
-        const int grid = gridTile[last ? MODE_LEAF : MODE_EXPAND][sv];
+        const int sv = lvSv[lv];
+        const int grid = lvGrid[lv];
         if (last) {
+            cudaEventRecord(G.evLeaf0, stream);
             if (sv == SV_KOGGE_SPLIT) k_tile<MODE_LEAF, SV_KOGGE_SPLIT, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
             else k_tile<MODE_LEAF, SV_KOGGE, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
+            cudaEventRecord(G.evLeaf1, stream);
         } else {
             if (sv == SV_KOGGE_SPLIT) k_tile<MODE_EXPAND, SV_KOGGE_SPLIT, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
             else k_tile<MODE_EXPAND, SV_KOGGE, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
+            const u32 nj = G.hTemplate->joinN[lv + 1];
+            if (nj) k_dd_join<<<(nj + 127) / 128, 128, 0, stream>>>(dPlan, lv + 1, G.dPos, dErr);
         }
     }
     cudaMemcpyAsync(&G.hFlags[0], &dPlan->overflow, 4, cudaMemcpyDeviceToHost, stream);
     cudaMemcpyAsync(&G.hFlags[1], dErr, 4, cudaMemcpyDeviceToHost, stream);
-    cudaMemcpyAsync(&G.hFlags[2], &dPlan->lv[d - 2].total, 8, cudaMemcpyDeviceToHost, stream);
+    if (d >= 2) {
+        cudaMemcpyAsync(&G.hFlags[2], &dPlan->lv[d - 2].total, 8, cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(&G.hFlags[3], &dPlan->lv[d - 2].n, 8, cudaMemcpyDeviceToHost, stream);
+    }
     const cudaError_t ce = cudaStreamEndCapture(stream, &G.graph);
     if (ce != cudaSuccess) {
         cudaGetLastError();
@@ -1666,32 +1789,51 @@ int Engine::build_dd(DDGraph &G)
     return PERFT_OK;
 }
 
-// Single-depth batches whose predicted tree is small run as one replayed
-// graph: the launch sequence is fixed and the sizes live on the device, so
-// the host only waits once.  `handled` stays false when the batch is not
-// eligible or the device plan overflowed; the caller then runs the
-// host-driven path.
+// Batches whose predicted tree fits the arena run as one replayed graph,
+// whatever their depth mix: the launch sequence is fixed and the sizes live
+// on the device, so the host only waits once.  The prediction charges each
+// root its own move count times 35 per further ply, 72 bytes per node of the
+// last materialised ply (planes, count, root, scan entry, tile index) and of
+// the plies above it, against 80% of the free arena.  `handled` stays false
+// when the batch is not eligible or the device plan overflowed; the caller
+// then runs the host-driven path.
 int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, bool &handled)
 {
     handled = false;
     if (!ddEnabled || tt || n == 0) return PERFT_OK;
-    const int d = depths[0];
-    for (u32 i = 1; i < n; i++)
-        if (depths[i] != d) return PERFT_OK;
-    if (d < 2 || d > DD_MAX_LEVELS) return PERFT_OK;
+    int d = 0;
+    for (u32 i = 0; i < n; i++) d = std::max<int>(d, depths[i]);
+    if (d > DD_MAX_LEVELS) return PERFT_OK;
     // the graph path has the two Kogge-Stone instantiations; another tuned
     // variant runs there as plain Kogge-Stone (same counts)
     auto ddSv = [](int v) { return (v == SV_KOGGE || v == SV_KOGGE_SPLIT) ? v : (int)SV_KOGGE; };
     const int ddL = ddSv(svLeaf), ddE = ddSv(svExpand);
-    double est = (double)n * 130.0;
-    for (int k = 2; k < d; k++) est *= 40.0;
-    if (est > 0.25 * (double)arena_free() && !ddForce) return PERFT_OK;
-
     DDGraph *G = nullptr;
     for (DDGraph &g : ddCache)
         if (g.depth == d && g.n == n && g.dPos == dPos && g.dOut == dOut && g.top == arenaTop && g.svL == ddL &&
-            g.svE == ddE)
+            g.svE == ddE && memcmp(g.depths.data(), depths, n) == 0)
             G = &g;
+    if (G && G->overflowed) return PERFT_OK;
+    if (!G && !ddForce) {
+        // Predicted bytes of the materialised plies: each root's own move
+        // count times 32 per further ply (the measured mean is about 30),
+        // 72 bytes per node.  The positions are read back once, when the
+        // graph is built; a replay needs no prediction.
+        std::vector<u64> hp(6ull * n);
+        ENG_TRY(cudaMemcpyAsync(hp.data(), dPos, 48ull * n, cudaMemcpyDeviceToHost, stream));
+        ENG_TRY(cudaStreamSynchronize(stream));
+        double est = 0;
+        for (u32 i = 0; i < n; i++) {
+            if (depths[i] < 2 || validate_pos48(&hp[6ull * i]) != 0) continue;
+            double nodes = (double)count_moves<SV_KOGGE>(from_pos48(&hp[6ull * i])), sum = 0;
+            for (int k = 1; k <= (int)depths[i] - 2; k++) {
+                sum += nodes;
+                nodes *= 32.0;
+            }
+            est += sum * 72.0;
+        }
+        if (est > 0.85 * (double)arena_free()) return PERFT_OK;
+    }
     if (!G) {
         if (ddCache.size() >= 16) {
             DDGraph &old = ddCache.front();
@@ -1700,11 +1842,14 @@ int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, boo
             cudaFreeHost(old.hTemplate);
             cudaFreeHost(old.hIds);
             cudaFreeHost(old.hFlags);
+            if (old.evLeaf0) cudaEventDestroy(old.evLeaf0);
+            if (old.evLeaf1) cudaEventDestroy(old.evLeaf1);
             ddCache.erase(ddCache.begin());
         }
         ddCache.emplace_back();
         G = &ddCache.back();
         G->depth = d;
+        G->depths.assign(depths, depths + n);
         G->n = n;
         G->dPos = dPos;
         G->dOut = dOut;
@@ -1717,17 +1862,26 @@ int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, boo
             return rc == PERFT_ERR_OUT_OF_MEMORY ? PERFT_OK : rc;
         }
     }
+    G->hFlags[2] = G->hFlags[3] = 0;
     ENG_TRY(cudaGraphLaunch(G->exec, stream));
     ENG_TRY(cudaStreamSynchronize(stream));
-    stats.other_launches += 1 + 3ull * (d - 1);
-    stats.expand_launches += d - 2;
-    stats.leaf_launches += 1;
+    stats.other_launches += 3 + 3ull * (d > 1 ? d - 1 : 0);
+    stats.expand_launches += d > 2 ? d - 2 : 0;
+    stats.leaf_launches += d >= 2 ? 1 : 0;
     stats.graph_launches += 1;
-    if ((u32)G->hFlags[0]) return PERFT_OK;  // overflow: rerun host-driven
+    if ((u32)G->hFlags[0]) {  // overflow: rerun host-driven, now and on later calls
+        G->overflowed = true;
+        return PERFT_OK;
+    }
     const u32 e = (u32)G->hFlags[1];
     if (e & DERR_BAD_POSITION) return PERFT_ERR_INVALID_ARG;
     if (e) return PERFT_ERR_INTERNAL;
     stats.leaf_items += G->hFlags[2];
+    stats.leaf_parents += G->hFlags[3];
+    if (d >= 2) {
+        float ms = 0.f;  // the count-only ply's device time, from the events recorded in the graph
+        if (cudaEventElapsedTime(&ms, G->evLeaf0, G->evLeaf1) == cudaSuccess) stats.leaf_ms += ms;
+    }
     handled = true;
     return PERFT_OK;
 }
@@ -1782,6 +1936,49 @@ int Engine::run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut)
     for (u32 i = 0; i < n; i++) groups[depths[i]].push_back(i);
 
     int rc = PERFT_OK;
+    if (!tt) {
+        // Without a table all depth groups share their plies: the deepest
+        // roots start, the others join the level of their remaining depth,
+        // so the batch takes one launch per ply (chunked only where a level
+        // does not fit the arena).  Roots of depth 0 and 1 are answered by
+        // k_init_roots alone.
+        std::vector<u32> order;
+        order.reserve(n);
+        Joiners J;
+        J.dPos = dPos;
+        std::vector<std::pair<int, size_t>> offs;
+        for (auto &g : groups) {
+            offs.push_back({g.first, order.size()});
+            order.insert(order.end(), g.second.begin(), g.second.end());
+        }
+        u32 *dIds = (u32 *)alloc(4ull * n);
+        if (!dIds) rc = PERFT_ERR_OUT_OF_MEMORY;
+        if (rc == PERFT_OK) {
+            ENG_TRY(cudaMemcpyAsync(dIds, order.data(), 4ull * n, cudaMemcpyHostToDevice, stream));
+            for (auto &o : offs) {
+                J.ids[o.first] = dIds + o.second;
+                J.n[o.first] = (u32)groups[o.first].size();
+            }
+            const int dmax = groups.begin()->first;
+            // the shallow roots (depth 0, 1) in one scratch level each
+            for (int d = 0; d <= 1 && rc == PERFT_OK; d++) {
+                if (!J.n[d]) continue;
+                const u64 gm = arenaTop;
+                DeviceLevel S;
+                if (!alloc_level(S, J.n[d])) rc = PERFT_ERR_OUT_OF_MEMORY;
+                else rc = init_joiners(J, d, S, 0, rootCounts);
+                arenaTop = gm;
+            }
+            if (rc == PERFT_OK && dmax >= 2) {
+                DeviceLevel L0;
+                if (!alloc_level(L0, J.n[dmax])) rc = PERFT_ERR_OUT_OF_MEMORY;
+                if (rc == PERFT_OK) rc = init_joiners(J, dmax, L0, 0, rootCounts);
+                if (rc == PERFT_OK) rc = sync_and_check_errors();
+                if (rc == PERFT_OK) rc = process_level(L0, dmax, rootCounts, &J);
+            }
+        }
+        groups.clear();  // done: skip the per-group loop below
+    }
     for (auto &g : groups) {
         const int depth = g.first;
         const std::vector<u32> &ids = g.second;

@@ -56,11 +56,23 @@ def _children(pg, pos):
     return np.stack([pg.apply_move(pos, m) for m in pg.legal_moves(pos)])
 
 
-def test_batch4096_every_position_equals_reference(big_engine, wl, cfg_golden):
-    want = np.array(cfg_golden["batch4096"]["counts"], dtype=np.uint64)
-    got = big_engine.perft_batch(wl["batch_pos"], wl["batch_depths"])
-    bad = np.nonzero(got != want)[0]
-    assert len(bad) == 0, [(int(i), int(got[i]), int(want[i])) for i in bad[:5]]
+@pytest.mark.parametrize("graphs", ["1", "0"], ids=["graph", "host_driven"])
+def test_batch4096_every_position_equals_reference(engine, wl, cfg_golden, graphs, monkeypatch):
+    """The whole batch as one captured graph (the default when its predicted
+    levels fit the arena) and host-driven."""
+    monkeypatch.setenv("PERFT_NO_GRAPHS", "0" if graphs == "1" else "1")
+    engine.init(device=0)
+    try:
+        want = np.array(cfg_golden["batch4096"]["counts"], dtype=np.uint64)
+        engine.reset_stats()
+        got = engine.perft_batch(wl["batch_pos"], wl["batch_depths"])
+        bad = np.nonzero(got != want)[0]
+        assert len(bad) == 0, [(int(i), int(got[i]), int(want[i])) for i in bad[:5]]
+        st = engine.stats()
+        assert st["leaf_launches"] == 1 and (st["graph_launches"] == 1) == (graphs == "1")
+    finally:
+        monkeypatch.delenv("PERFT_NO_GRAPHS")
+        engine.init(device=0, arena_bytes=8 << 30)
 
 
 def test_deep_position_divided_perft8_equals_reference(big_engine, wl, cfg_golden):

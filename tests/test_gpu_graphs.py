@@ -59,3 +59,35 @@ def test_graph_overflow_falls_back(engine, golden):
         else:
             os.environ["PERFT_DD_FORCE"] = old
         engine.init(device=0, arena_bytes=8 << 30)
+
+
+def test_mixed_depth_batch_as_one_graph(engine, oracle):
+    """A batch of depths 0-5 runs as one graph (deepest roots start, the
+    others join the ply of their remaining depth) and equals the host-driven
+    path and the oracle; the host-driven path also shares plies across depth
+    groups."""
+    pos = engine.random_playouts(seed=72, n=120, min_plies=0, max_plies=40)
+    depths = (np.arange(len(pos)) * 7 % 6).astype(np.uint8)  # 0..5, interleaved
+    want = oracle.perft_batch_mt(pos, depths)
+    try:
+        _reinit(engine, PERFT_NO_GRAPHS="1")
+        engine.reset_stats()
+        host = engine.perft_batch(pos, depths)
+        st = engine.stats()
+        assert st["graph_launches"] == 0
+        assert st["leaf_launches"] == 1  # every depth group in one count-only launch
+        assert np.array_equal(host, want)
+        _reinit(engine, PERFT_NO_GRAPHS="0")
+        engine.reset_stats()
+        for _ in range(2):
+            assert np.array_equal(engine.perft_batch(pos, depths), want)
+        st = engine.stats()
+        assert st["graph_launches"] == 2
+        assert st["leaf_ms"] > 0 and st["leaf_items"] > 0 and st["leaf_parents"] > 0  # timed inside the graph
+        # a depth mix with an empty join level and shallow roots only
+        d2 = np.where(depths >= 3, 5, depths % 2).astype(np.uint8)
+        assert np.array_equal(engine.perft_batch(pos, d2), oracle.perft_batch_mt(pos, d2))
+        d3 = (depths % 2).astype(np.uint8)
+        assert np.array_equal(engine.perft_batch(pos, d3), oracle.perft_batch_mt(pos, d3))
+    finally:
+        engine.init(device=0, arena_bytes=8 << 30)
