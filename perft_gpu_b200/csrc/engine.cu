@@ -573,7 +573,7 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
             if (valid && qEnd > qBeg && qEnd > sBeg && qBeg < sEnd) {
                 const Board b{sb[0][tid], sb[1][tid], sb[2][tid], sb[3][tid], sb[4][tid], sb[5][tid]};
                 WindowSink sink{sitems, (int)((long long)qBeg - (long long)sBeg), (u32)(sEnd - sBeg), (u32)tid << 16};
-                gen_moves<SV>(b, sink);
+                gen_moves<SV, true>(b, sink);  // items carry the mover's planes (make_child<true>)
                 if ((long long)sink.rel != (long long)qEnd - (long long)sBeg) atomicOr(P.err, DERR_GEN_MISMATCH);
             }
             __syncthreads();
@@ -586,11 +586,11 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
                 u32 cnt = 0;
                 int pl = 0;
                 if (act) {
-                    const u32 it = sitems[j];
-                    pl = (int)(it >> 16);
+                    const u32 it = sitems[j];  // move (bits 0-15), parent slot (16-23), mover planes (24-28)
+                    pl = (int)((it >> 16) & 0xFFu);
                     if (pl < nP) {
                         const Board b{sb[0][pl], sb[1][pl], sb[2][pl], sb[3][pl], sb[4][pl], sb[5][pl]};
-                        const Board ch = make_child(b, it & 0xFFFFu);
+                        const Board ch = make_child<true>(b, it);
                         cnt = count_moves<SV>(ch);
                         if (MODE == MODE_EXPAND) {
                             const u64 g = sBeg + (u64)j - P.itemBase;

@@ -915,6 +915,7 @@ PG_HD u32 count_moves(const Board &b)
 }
 
 // ---------------------------------------------------------------- generate
+// `from` may carry mover bits (bits 24-28) above the square.
 PG_HD u32 encode_move(int from, int to, u32 flags)
 {
     return (flags << 12) | ((u32)to << 6) | (u32)from;
@@ -942,9 +943,16 @@ PG_HD void emit_pawn(Sink &out, int from, int to, u32 flags)
     }
 }
 
+// Mover bits (MOVER = true): each emitted move also carries, in bits 24-28,
+// the planes the moving piece occupies (pawn 1, knight 2, bishop/queen 4,
+// rook/queen 8, king 16), so make_child<true> needs no piece lookup.  The
+// generator knows the piece of every move it emits, so the bits cost one OR
+// per piece, not per move.
+enum : u32 { MV_P = 1u << 24, MV_N = 2u << 24, MV_BQ = 4u << 24, MV_RQ = 8u << 24, MV_K = 16u << 24 };
+
 // Generates every legal move of the side to move.  Emits exactly
 // count_moves<SV>(b) moves.
-template <int SV, class Sink>
+template <int SV, bool MOVER = false, class Sink>
 PG_HD void gen_moves(const Board &b, Sink &out)
 {
     // per-piece targets: one magic lookup per slider beats a single-bit
@@ -954,15 +962,16 @@ PG_HD void gen_moves(const Board &b, Sink &out)
     Ctx c;
     setup_ctx<PG_GEN_MAGIC_ATTACKS ? GEN_SV : SV>(b, c);
     const u64 notMine = ~c.mine;
-    emit_targets(out, c.ksq, PG_TAB(king[c.ksq]) & notMine & ~c.attacked);
+    const u32 mvP = MOVER ? MV_P : 0, mvN = MOVER ? MV_N : 0, mvK = MOVER ? MV_K : 0;
+    emit_targets(out, c.ksq | mvK, PG_TAB(king[c.ksq]) & notMine & ~c.attacked);
     const u64 cm = check_mask<SV>(c);
     if (!cm) return;
     const bool inCheck = cm != ~0ULL;
     const u64 targets = notMine & cm;
 
     if (!inCheck) {
-        if ((c.st & 1) && !((c.occ | c.attacked) & 0x60ULL)) out(encode_move(4, 6, MF_KING_CASTLE));
-        if ((c.st & 2) && !(c.occ & 0x0EULL) && !(c.attacked & 0x0CULL)) out(encode_move(4, 2, MF_QUEEN_CASTLE));
+        if ((c.st & 1) && !((c.occ | c.attacked) & 0x60ULL)) out(encode_move(4 | mvK, 6, MF_KING_CASTLE));
+        if ((c.st & 2) && !(c.occ & 0x0EULL) && !(c.attacked & 0x0CULL)) out(encode_move(4 | mvK, 2, MF_QUEEN_CASTLE));
     }
 
     const u64 pinned = pinned_of(c);
@@ -975,33 +984,40 @@ PG_HD void gen_moves(const Board &b, Sink &out)
         if (p & c.pawns) {
             const u64 p1 = sh_n(p) & c.empty & line;
             if (p1) {
-                out(encode_move(s, s + 8, MF_QUIET));
-                if (sh_n(p1 & RANK3) & c.empty) out(encode_move(s, s + 16, MF_DOUBLE_PUSH));
+                out(encode_move(s | mvP, s + 8, MF_QUIET));
+                if (sh_n(p1 & RANK3) & c.empty) out(encode_move(s | mvP, s + 16, MF_DOUBLE_PUSH));
             }
             const u64 cap = pawn_att_up(p) & line & c.theirs;
-            if (cap) emit_pawn(out, s, ctz(cap), MF_CAPTURE);
+            if (cap) emit_pawn(out, s | mvP, ctz(cap), MF_CAPTURE);
             return;
         }
         u64 t = 0;
         if (p & b.bq) t |= bishop_att<GEN_SV>(s, c.occ);
         if (p & b.rq) t |= rook_att<GEN_SV>(s, c.occ);
-        emit_targets(out, s, t & notMine & line);
+        const u32 mv = MOVER ? (((p & b.bq) ? MV_BQ : 0u) | ((p & b.rq) ? MV_RQ : 0u)) : 0u;
+        emit_targets(out, s | mv, t & notMine & line);
     });
 
     // free pieces
-    for_each_bit(b.knights & c.mine & ~pinned, [&](int s) { emit_targets(out, s, PG_TAB(knight[s]) & targets); });
-    for_each_bit(b.bq & c.mine & ~pinned,
-                 [&](int s) { emit_targets(out, s, bishop_att<GEN_SV>(s, c.occ) & targets); });
-    for_each_bit(b.rq & c.mine & ~pinned, [&](int s) { emit_targets(out, s, rook_att<GEN_SV>(s, c.occ) & targets); });
+    for_each_bit(b.knights & c.mine & ~pinned,
+                 [&](int s) { emit_targets(out, s | mvN, PG_TAB(knight[s]) & targets); });
+    for_each_bit(b.bq & c.mine & ~pinned, [&](int s) {
+        const u32 mv = MOVER ? (MV_BQ | (((b.rq >> s) & 1) ? MV_RQ : 0u)) : 0u;  // a queen is on both planes
+        emit_targets(out, s | mv, bishop_att<GEN_SV>(s, c.occ) & targets);
+    });
+    for_each_bit(b.rq & c.mine & ~pinned, [&](int s) {
+        const u32 mv = MOVER ? (MV_RQ | (((b.bq >> s) & 1) ? MV_BQ : 0u)) : 0u;
+        emit_targets(out, s | mv, rook_att<GEN_SV>(s, c.occ) & targets);
+    });
     const u64 P = c.pawns & c.mine & ~pinned;
     const u64 p1 = sh_n(P) & c.empty;
     u64 p1c = p1 & cm;
     u64 p2 = sh_n(p1 & RANK3) & c.empty & cm;
-    for_each_bit(p1c, [&](int to) { emit_pawn(out, to - 8, to, MF_QUIET); });
-    for_each_bit(p2, [&](int to) { out(encode_move(to - 16, to, MF_DOUBLE_PUSH)); });
+    for_each_bit(p1c, [&](int to) { emit_pawn(out, (to - 8) | mvP, to, MF_QUIET); });
+    for_each_bit(p2, [&](int to) { out(encode_move((to - 16) | mvP, to, MF_DOUBLE_PUSH)); });
     const u64 capT = c.theirs & cm;
-    for_each_bit(sh_nw(P) & capT, [&](int to) { emit_pawn(out, to - 7, to, MF_CAPTURE); });
-    for_each_bit(sh_ne(P) & capT, [&](int to) { emit_pawn(out, to - 9, to, MF_CAPTURE); });
+    for_each_bit(sh_nw(P) & capT, [&](int to) { emit_pawn(out, (to - 7) | mvP, to, MF_CAPTURE); });
+    for_each_bit(sh_ne(P) & capT, [&](int to) { emit_pawn(out, (to - 9) | mvP, to, MF_CAPTURE); });
     const u32 epf = c.st >> 4;
     if (epf) {
         const u64 target = 1ULL << (39 + epf);
@@ -1013,7 +1029,7 @@ PG_HD void gen_moves(const Board &b, Sink &out)
                 srcs ^= s;
                 const bool ok = (s & pinned) ? (!inCheck && (PG_TAB(line[ctz(s)][c.ksq]) & target) != 0)
                                              : !ep_exposes_king(c, s, captured);
-                if (ok) out(encode_move(ctz(s), 39 + epf, MF_EP));
+                if (ok) out(encode_move(ctz(s) | mvP, 39 + epf, MF_EP));
             }
         }
     }
@@ -1022,6 +1038,10 @@ PG_HD void gen_moves(const Board &b, Sink &out)
 // ------------------------------------------------------------------- make
 // Applies a legal move and returns the child from the opponent's point of
 // view (mirrored).  Branch-free except for the flag decode.
+// With MOVER, mv carries the mover bits of gen_moves<SV, true> (bits 24-28)
+// and the piece planes of the moving piece are not looked up; bits 16-23 are
+// ignored either way.
+template <bool MOVER = false>
 PG_HD Board make_child(const Board &b, u32 mv)
 {
     const int from = mv & 63, to = (mv >> 6) & 63;
@@ -1031,11 +1051,11 @@ PG_HD Board make_child(const Board &b, u32 mv)
     const u64 pawns0 = b.pawns & RANKS2TO7;
     const u64 theirPawns = pawns0 & ~b.mine;
 
-    const u64 mP = maskIf((pawns0 >> from) & 1);
-    const u64 mN = maskIf((b.knights >> from) & 1);
-    const u64 mB = maskIf((b.bq >> from) & 1);
-    const u64 mR = maskIf((b.rq >> from) & 1);
-    const u64 mK = maskIf((b.kings >> from) & 1);
+    const u64 mP = MOVER ? maskIf(mv & MV_P) : maskIf((pawns0 >> from) & 1);
+    const u64 mN = MOVER ? maskIf(mv & MV_N) : maskIf((b.knights >> from) & 1);
+    const u64 mB = MOVER ? maskIf(mv & MV_BQ) : maskIf((b.bq >> from) & 1);
+    const u64 mR = MOVER ? maskIf(mv & MV_RQ) : maskIf((b.rq >> from) & 1);
+    const u64 mK = MOVER ? maskIf(mv & MV_K) : maskIf((b.kings >> from) & 1);
 
     u64 pawns = pawns0 & ~sd;
     u64 kn = b.knights & ~sd;

@@ -74,6 +74,24 @@ uint32_t hc_children(const uint64_t pos[6], int sv, uint64_t *out)
     return s.n;
 }
 
+// Children as the tile kernel makes them: moves carrying the mover's planes
+// (gen_moves<SV, true>), children made without piece lookups
+// (make_child<true>), with a parent slot in bits 16-23 as the kernel's items
+// have.  Also writes the 16-bit moves to mv16.
+uint32_t hc_children_mover(const uint64_t pos[6], int sv, uint64_t *out, uint16_t *mv16)
+{
+    const Board b = from_pos48(pos);
+    u32 moves[256];
+    VecSink s{moves, 0};
+    with_sv(sv, [&]<int SV>() { gen_moves<SV, true>(b, s); return 0; });
+    for (u32 i = 0; i < s.n; i++) {
+        Board c = make_child<true>(b, moves[i] | (0xA5u << 16));
+        to_pos48(c, out + 6 * i);
+        mv16[i] = (uint16_t)moves[i];
+    }
+    return s.n;
+}
+
 uint64_t hc_perft(const uint64_t pos[6], uint32_t depth, int sv)
 {
     const Board b = from_pos48(pos);

@@ -90,3 +90,29 @@ def test_stratified_batch_sample_vs_oracle(hc, oracle, sv):
         assert hc.hc_count(pp, sv) == len(kids)
         assert _children(hc, p, sv) == sorted(tuple(int(x) for x in k) for k in kids)
         assert hc.hc_perft(pp, 2, sv) == oracle.perft(p, 2)
+
+
+@pytest.mark.parametrize("sv", SV_ALL, ids=SV_IDS)
+def test_mover_bits_children(hc, golden, sv):
+    """Moves that carry the mover's planes (the tile kernel's items) give the
+    same 16-bit moves in the same order and the same children as plain
+    generation with piece lookups in make-move."""
+    hc.hc_children_mover.restype = ctypes.c_uint32
+    pos = [pos48_from_hex(e["pos48"]) for e in golden]
+    rng = random.Random(5)
+    buf = (ctypes.c_uint64 * (6 * 256))()
+    for p in pos:
+        # walk a few plies from each golden position
+        for _ in range(12):
+            kids = _children(hc, p, sv)
+            n = len(kids)
+            mv = (ctypes.c_uint16 * 256)()
+            m = hc.hc_children_mover(P6(*[int(x) for x in p]), sv, buf, mv)
+            assert m == n
+            assert sorted(tuple(buf[6 * i:6 * i + 6]) for i in range(m)) == kids
+            plain = (ctypes.c_uint64 * (6 * 256))()
+            hc.hc_children(P6(*[int(x) for x in p]), sv, plain)
+            assert [tuple(buf[6 * i:6 * i + 6]) for i in range(m)] == [tuple(plain[6 * i:6 * i + 6]) for i in range(n)]
+            if n == 0:
+                break
+            p = np.array(kids[rng.randrange(n)], dtype=np.uint64)
