@@ -573,7 +573,7 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
             if (valid && qEnd > qBeg && qEnd > sBeg && qBeg < sEnd) {
                 const Board b{sb[0][tid], sb[1][tid], sb[2][tid], sb[3][tid], sb[4][tid], sb[5][tid]};
                 WindowSink sink{sitems, (int)((long long)qBeg - (long long)sBeg), (u32)(sEnd - sBeg), (u32)tid << 16};
-                gen_moves<SV, true>(b, sink);  // items carry the mover's planes (make_child<true>)
+                gen_moves<SV, PG_MOVER_BITS>(b, sink);  // items carry the mover's planes
                 if ((long long)sink.rel != (long long)qEnd - (long long)sBeg) atomicOr(P.err, DERR_GEN_MISMATCH);
             }
             __syncthreads();
@@ -590,7 +590,7 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
                     pl = (int)((it >> 16) & 0xFFu);
                     if (pl < nP) {
                         const Board b{sb[0][pl], sb[1][pl], sb[2][pl], sb[3][pl], sb[4][pl], sb[5][pl]};
-                        const Board ch = make_child<true>(b, it);
+                        const Board ch = make_child<PG_MOVER_BITS>(b, it);
                         cnt = count_moves<SV>(ch);
                         if (MODE == MODE_EXPAND) {
                             const u64 g = sBeg + (u64)j - P.itemBase;
@@ -1763,10 +1763,12 @@ int Engine::build_dd(DDGraph &G)
         const int sv = lvSv[lv];
         const int grid = lvGrid[lv];
         if (last) {
-            cudaEventRecord(G.evLeaf0, stream);
+            // external records: event record nodes in the graph (a plain
+            // record during capture only orders the capture)
+            cudaEventRecordWithFlags(G.evLeaf0, stream, cudaEventRecordExternal);
             if (sv == SV_KOGGE_SPLIT) k_tile<MODE_LEAF, SV_KOGGE_SPLIT, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
             else k_tile<MODE_LEAF, SV_KOGGE, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
-            cudaEventRecord(G.evLeaf1, stream);
+            cudaEventRecordWithFlags(G.evLeaf1, stream, cudaEventRecordExternal);
         } else {
             if (sv == SV_KOGGE_SPLIT) k_tile<MODE_EXPAND, SV_KOGGE_SPLIT, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
             else k_tile<MODE_EXPAND, SV_KOGGE, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
@@ -1881,6 +1883,7 @@ int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, boo
     if (d >= 2) {
         float ms = 0.f;  // the count-only ply's device time, from the events recorded in the graph
         if (cudaEventElapsedTime(&ms, G->evLeaf0, G->evLeaf1) == cudaSuccess) stats.leaf_ms += ms;
+        else cudaGetLastError();  // a statistic only: leave no error behind for the caller
     }
     handled = true;
     return PERFT_OK;

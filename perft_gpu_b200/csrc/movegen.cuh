@@ -66,6 +66,11 @@
 #ifndef PG_GEN_MAGIC
 #define PG_GEN_MAGIC 1
 #endif
+// PG_MOVER_BITS 1: the tile kernel's generated items carry the moving
+// piece's planes, so its make-move needs no piece lookups.
+#ifndef PG_MOVER_BITS
+#define PG_MOVER_BITS 1
+#endif
 // PG_GEN_MAGIC_ATTACKS 1: generation also builds the opponent's attack map
 // from magic lookups, one per opponent slider.
 #ifndef PG_GEN_MAGIC_ATTACKS
