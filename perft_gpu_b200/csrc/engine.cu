@@ -320,6 +320,8 @@ __global__ void __launch_bounds__(SCAN_NT) k_dd_scan_reduce(DevPlan *plan, int l
     }
 }
 
+__device__ void dd_plan_level(DevPlan *plan, int lv, int last, u64 total);
+
 __global__ void __launch_bounds__(SCAN_TOP_NT) k_dd_scan_top(DevPlan *plan, int lv, int last)
 {
     __shared__ u64 sw[SCAN_TOP_NT / 32];
@@ -336,7 +338,54 @@ __global__ void __launch_bounds__(SCAN_TOP_NT) k_dd_scan_top(DevPlan *plan, int 
         L.bsum[i] = run;
         run += v;
     }
-    if (threadIdx.x != 0) return;
+    if (threadIdx.x == 0) dd_plan_level(plan, lv, last, total);
+}
+
+// Whole-level scan in one block: the total, the tile size and the next level
+// (dd_plan_level), then the offsets and tile index, 1024 nodes per pass.
+// Used for levels predicted small, where three launches (each with its own
+// latency) would cost more than the work; correct for any size.
+__global__ void __launch_bounds__(1024) k_dd_scan_small(DevPlan *plan, int lv, int last)
+{
+    __shared__ u64 sw[32];
+    __shared__ int sCap;
+    LevelDesc &L = plan->lv[lv];
+    const u64 n = L.n;
+    u64 s = 0;
+    for (u64 i = threadIdx.x; i < n; i += 1024) s += L.cnt[i];
+    u64 total;
+    block_excl_scan_u64<1024>(s, sw, total);
+    if (threadIdx.x == 0) {
+        dd_plan_level(plan, lv, last, total);
+        sCap = L.capLog2;
+    }
+    __syncthreads();
+    const int cl = sCap;
+    u64 base = 0;
+    for (u64 c0 = 0; c0 < n; c0 += 1024) {
+        const u64 i = c0 + threadIdx.x;
+        const u32 c = i < n ? L.cnt[i] : 0u;
+        u64 tot;
+        const u64 run = base + block_excl_scan_u64<1024>(c, sw, tot);
+        if (i < n) {
+            L.pscan[i] = run;
+            if (c) {
+                const u64 t0 = (run + (1ull << cl) - 1) >> cl;
+                const u64 t1 = (run + c - 1) >> cl;
+                for (u64 t = t0; t <= t1; t++) L.tileFirst[t] = (u32)i;
+            }
+        }
+        base += tot;
+    }
+}
+
+// Top-of-scan bookkeeping of a device-driven level (one thread): the level's
+// total and tile size, then the next level's buffers from the plan's bump
+// allocator (children plus the roots joining there).
+__device__ void dd_plan_level(DevPlan *plan, int lv, int last, u64 total)
+{
+    LevelDesc &L = plan->lv[lv];
+    const u64 n = L.n;
     if (n) L.pscan[n] = total;
     L.total = plan->overflow ? 0 : total;
     int cap = plan->capMax[lv] ? plan->capMax[lv] : TILE_CAP_LOG2;
@@ -472,26 +521,37 @@ struct WindowSink {
 template <int MODE, int SV, bool TRACK = false, bool DD = false>
 __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pin)
 {
-    TileParams P = Pin;
+    // Device-driven runs take the level pointers and sizes from the plan.
+    // They are kept in shared memory, not in registers: held in registers
+    // across the make-and-count loop they cost the count registers (the
+    // kernel runs at the 80-register cap), which measured 5% slower.  Plain
+    // launches read them from the parameter bank.
+    __shared__ TileParams sP;
     if (DD) {
-        const LevelDesc &a = *Pin.dpar;
-        P.ppl = a.planes;
-        P.pstride = a.stride;
-        P.pscan = a.pscan;
-        P.proot = a.root;
-        P.nParents = a.n;
-        P.tileFirst = a.tileFirst;
-        P.itemBase = 0;
-        P.itemEnd = a.total;
-        P.capLog2 = a.capLog2;
-        if (MODE == MODE_EXPAND) {
-            const LevelDesc &c = *Pin.dch;
-            P.cpl = c.planes;
-            P.cstride = c.stride;
-            P.ccnt = c.cnt;
-            P.croot = c.root;
+        if (threadIdx.x == 0) {
+            TileParams q = Pin;
+            const LevelDesc &a = *Pin.dpar;
+            q.ppl = a.planes;
+            q.pstride = a.stride;
+            q.pscan = a.pscan;
+            q.proot = a.root;
+            q.nParents = a.n;
+            q.tileFirst = a.tileFirst;
+            q.itemBase = 0;
+            q.itemEnd = a.total;
+            q.capLog2 = a.capLog2;
+            if (MODE == MODE_EXPAND) {
+                const LevelDesc &c = *Pin.dch;
+                q.cpl = c.planes;
+                q.cstride = c.stride;
+                q.ccnt = c.cnt;
+                q.croot = c.root;
+            }
+            sP = q;
         }
+        __syncthreads();
     }
+    const TileParams &P = DD ? sP : Pin;
     __shared__ u64 sb[6][TILE_MAXP];
     __shared__ u64 sqEnd[TRACK ? TILE_MAXP : 1];
     __shared__ int sdelta[TRACK ? TILE_MAXP : 1];
@@ -1016,6 +1076,7 @@ private:
         int svL = 0, svE = 0;
         bool overflowed = false;  // the plan did not fit: later calls go host-driven at once
         cudaEvent_t evLeaf0 = nullptr, evLeaf1 = nullptr;  // recorded around the count-only ply
+        std::vector<double> predLv;  // predicted nodes per level (empty: no prediction)
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         DevPlan *hTemplate = nullptr;  // pinned
@@ -1749,9 +1810,14 @@ int Engine::build_dd(DDGraph &G)
                                                                       (unsigned long long *)G.dOut, dErr);
     for (int lv = 0; lv <= d - 2; lv++) {
         const int last = lv == d - 2;
-        k_dd_scan_reduce<<<ddGridScan, SCAN_NT, 0, stream>>>(dPlan, lv);
-        k_dd_scan_top<<<1, SCAN_TOP_NT, 0, stream>>>(dPlan, lv, last);
-        k_dd_scan_apply<<<ddGridScan, SCAN_NT, 0, stream>>>(dPlan, lv);
+        // levels predicted small take one single-block scan launch instead of three
+        if ((int)G.predLv.size() > lv && G.predLv[lv] <= 32768.0) {
+            k_dd_scan_small<<<1, 1024, 0, stream>>>(dPlan, lv, last);
+        } else {
+            k_dd_scan_reduce<<<ddGridScan, SCAN_NT, 0, stream>>>(dPlan, lv);
+            k_dd_scan_top<<<1, SCAN_TOP_NT, 0, stream>>>(dPlan, lv, last);
+            k_dd_scan_apply<<<ddGridScan, SCAN_NT, 0, stream>>>(dPlan, lv);
+        }
         cudaMemsetAsync(dCounter, 0, 4, stream);
         TileParams P;
         memset(&P, 0, sizeof P);
@@ -1816,6 +1882,7 @@ int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, boo
             g.svE == ddE && memcmp(g.depths.data(), depths, n) == 0)
             G = &g;
     if (G && G->overflowed) return PERFT_OK;
+    std::vector<double> predLv;
     if (!G && !ddForce) {
         // Predicted bytes of the materialised plies: each root's own move
         // count times 32 per further ply (the measured mean is about 30),
@@ -1825,11 +1892,15 @@ int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, boo
         ENG_TRY(cudaMemcpyAsync(hp.data(), dPos, 48ull * n, cudaMemcpyDeviceToHost, stream));
         ENG_TRY(cudaStreamSynchronize(stream));
         double est = 0;
+        predLv.assign(DD_MAX_LEVELS, 0.0);
         for (u32 i = 0; i < n; i++) {
             if (depths[i] < 2 || validate_pos48(&hp[6ull * i]) != 0) continue;
+            const int join = d - depths[i];  // the level this root enters
+            predLv[join] += 1.0;
             double nodes = (double)count_moves<SV_KOGGE>(from_pos48(&hp[6ull * i])), sum = 0;
             for (int k = 1; k <= (int)depths[i] - 2; k++) {
                 sum += nodes;
+                predLv[join + k] += nodes;
                 nodes *= 32.0;
             }
             est += sum * 72.0;
@@ -1858,6 +1929,7 @@ int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, boo
         G->top = arenaTop;
         G->svL = ddL;
         G->svE = ddE;
+        G->predLv = predLv;
         const int rc = build_dd(*G);
         if (rc != PERFT_OK) {
             drop_dd();
