@@ -58,9 +58,10 @@ def _children(pg, pos):
 
 @pytest.mark.parametrize("graphs", ["1", "0"], ids=["graph", "host_driven"])
 def test_batch4096_every_position_equals_reference(engine, wl, cfg_golden, graphs, monkeypatch):
-    """The whole batch as one captured graph (the default when its predicted
-    levels fit the arena) and host-driven."""
+    """The whole batch host-driven (the default for a tree this large) and as
+    one captured graph (allowed here up to the whole arena)."""
     monkeypatch.setenv("PERFT_NO_GRAPHS", "0" if graphs == "1" else "1")
+    monkeypatch.setenv("PERFT_DD_MAX_GB", "1000")
     engine.init(device=0)
     try:
         want = np.array(cfg_golden["batch4096"]["counts"], dtype=np.uint64)
@@ -72,6 +73,7 @@ def test_batch4096_every_position_equals_reference(engine, wl, cfg_golden, graph
         assert st["leaf_launches"] == 1 and (st["graph_launches"] == 1) == (graphs == "1")
     finally:
         monkeypatch.delenv("PERFT_NO_GRAPHS")
+        monkeypatch.delenv("PERFT_DD_MAX_GB")
         engine.init(device=0, arena_bytes=8 << 30)
 
 
