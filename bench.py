@@ -414,7 +414,9 @@ def measure_configs(args, pg, device, d_pos, depths, batch_ms_per_step, golden):
         "workload": BATCH_DESC.format(n=n) + ", with a 2^%d-entry table cleared before the step" % args.tt_log2,
         "steps": 1, "ms_per_step": ms, "value": float(got.sum()) / (ms / 1e3),
         "unit": UNIT + " (effective: leaves counted)",
-        "equals_reference": bool(np.array_equal(got, want)) if want is not None else None, "clocks": clk}
+        "equals_reference": bool(np.array_equal(got, want)) if want is not None else None,
+        # the same leaves against the plain one-position-per-call form (no table)
+        "over_single_plain": out["batch4096_single"]["ms_per_step"] / ms if ms > 0 else None, "clocks": clk}
     return out
 
 
