@@ -47,11 +47,6 @@
 #ifndef PG_KNIGHT_LUT
 #define PG_KNIGHT_LUT 1
 #endif
-// PG_OPP_KNIGHT_LUT: the fused count's opponent knight attacks; 0 = eight
-// jump shifts over the knight set, 1 = one table lookup per knight.
-#ifndef PG_OPP_KNIGHT_LUT
-#define PG_OPP_KNIGHT_LUT 0
-#endif
 // PG_KS_LINE 1: the fused count fills both directions of a line from one
 // propagator chain.
 #ifndef PG_KS_LINE
@@ -750,12 +745,7 @@ PG_HD u32 count_moves_fused(const Board &b)
         ks_pair<9, false, M>(tB, B, empty, ~FILEH, targets, attacked, n);
 #endif
     }
-    if (PG_OPP_KNIGHT_LUT) {
-        for_each_bit(tN, [&](int sq) { attacked |= PG_TAB(knight[sq]); });
-        attacked |= pawn_att_down(tP) | PG_TAB(king[ctz(b.kings & theirs)]);
-    } else {
-        attacked |= pawn_att_down(tP) | knight_set_att(tN) | PG_TAB(king[ctz(b.kings & theirs)]);
-    }
+    attacked |= pawn_att_down(tP) | knight_set_att(tN) | PG_TAB(king[ctz(b.kings & theirs)]);
 
     // king
     n += popc(PG_TAB(king[ksq]) & notMine & ~(attacked | xray));

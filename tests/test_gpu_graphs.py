@@ -91,3 +91,26 @@ def test_mixed_depth_batch_as_one_graph(engine, oracle):
         assert np.array_equal(engine.perft_batch(pos, d3), oracle.perft_batch_mt(pos, d3))
     finally:
         engine.init(device=0, arena_bytes=8 << 30)
+
+
+def test_mixed_depth_graph_overflow_falls_back(engine, oracle):
+    """With the size prediction disabled and a 64 MiB arena, the plan for a
+    mixed batch whose deepest roots need more overflows part-way (after
+    roots have joined); the host-driven path recomputes every count, and the
+    same call again goes host-driven at once."""
+    import os
+    pos = engine.random_playouts(seed=73, n=24, min_plies=4, max_plies=30)
+    depths = np.array([6 if i < 2 else 2 + i % 4 for i in range(len(pos))], dtype=np.uint8)
+    want = oracle.perft_batch_mt(pos, depths)
+    old = os.environ.get("PERFT_DD_FORCE")
+    os.environ["PERFT_DD_FORCE"] = "1"
+    try:
+        engine.init(device=0, arena_bytes=64 << 20)
+        for _ in range(2):
+            assert np.array_equal(engine.perft_batch(pos, depths), want)
+    finally:
+        if old is None:
+            os.environ.pop("PERFT_DD_FORCE", None)
+        else:
+            os.environ["PERFT_DD_FORCE"] = old
+        engine.init(device=0, arena_bytes=8 << 30)
