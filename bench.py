@@ -287,12 +287,15 @@ def run_reference(args):
     if rank != 0:
         return 0
     pos, depths, cfg, _ = make_workload(args.workload, 0, args.positions)
+    # each timed step is a bounded sample; the whole run stays within about
+    # three minutes however many steps are asked for
+    per_step = min(args.cpu_seconds, max(2.0, 150.0 / max(1, args.steps)))
     vals = []
     for _ in range(args.warmup):
-        cpu_sample(pos, depths, min(3.0, args.cpu_seconds))
+        cpu_sample(pos, depths, min(3.0, per_step))
     last = None
     for _ in range(args.steps):
-        last = cpu_sample(pos, depths, args.cpu_seconds)
+        last = cpu_sample(pos, depths, per_step)
         vals.append(last["value"])
     v = float(np.mean(vals))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
