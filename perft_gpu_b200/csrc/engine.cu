@@ -63,6 +63,9 @@ namespace {
 #ifndef PG_ONE_RUN_VOTE
 #define PG_ONE_RUN_VOTE 1  // one block vote for windows whose parents share one root
 #endif
+#ifndef PG_ONE_RUN_SUM
+#define PG_ONE_RUN_SUM 1  // such windows sum their counts with a plain warp reduction
+#endif
 #ifndef PG_TILE_NT
 #define PG_TILE_NT 256
 #endif
@@ -666,7 +669,12 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
                         pl = 0;
                     }
                 }
-                if (MODE == MODE_LEAF || TRACK) {
+                if (PG_ONE_RUN_SUM && MODE == MODE_LEAF && !TRACK && nRuns == 1) {
+                    // the whole window belongs to one root: a plain warp sum
+                    // (idle lanes hold 0), no grouping by root
+                    const u32 sum = __reduce_add_sync(0xffffffffu, cnt);
+                    if (lane == 0 && sum) atomicAdd(&sacc[0], (unsigned long long)sum);
+                } else if (MODE == MODE_LEAF || TRACK) {
                     const u32 key = act ? srun[pl] : 0xFFFFFFFFu;
                     const unsigned peers = __match_any_sync(0xffffffffu, key);
                     if (MODE == MODE_LEAF) {

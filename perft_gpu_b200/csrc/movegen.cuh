@@ -47,6 +47,11 @@
 #ifndef PG_KNIGHT_LUT
 #define PG_KNIGHT_LUT 1
 #endif
+// PG_COUNT_TABLES 1: the fused count takes a king's pawn checkers and each
+// pin line's length and kind from tables instead of computing them.
+#ifndef PG_COUNT_TABLES
+#define PG_COUNT_TABLES 1
+#endif
 // PG_KS_LINE 1: the fused count fills both directions of a line from one
 // propagator chain.
 #ifndef PG_KS_LINE
@@ -147,6 +152,8 @@ struct Tables {
     u64 rookMagic[64], bishopMagic[64];
     u32 rookOffset[64], bishopOffset[64];
     u32 rookShift[64], bishopShift[64];
+    u64 pawnUp[64];         // squares a side-to-move pawn on s attacks (its checkers of a king on s)
+    uint8_t pairInfo[64][64];  // squares strictly between (bits 0-2) and 8 when the line is a diagonal
 };
 
 // Total entries of the fancy-magic attack table (rook part then bishop part).
@@ -677,9 +684,11 @@ PG_HD u32 count_moves_fused(const Board &b)
         }
         if ((blk & (blk - 1)) || !(blk & mine)) return;
         pinned |= blk;
-        const bool diag = ((ksq ^ s) & 7) != 0 && ((ksq ^ s) >> 3) != 0;  // neither same file nor same rank
+        const u32 info = PG_COUNT_TABLES ? PG_TAB(pairInfo[ksq][s]) : 0u;
+        const bool diag = PG_COUNT_TABLES ? (info & 8) != 0
+                                          : (((ksq ^ s) & 7) != 0 && ((ksq ^ s) >> 3) != 0);  // neither file nor rank
         if (blk & (diag ? b.bq : b.rq)) {
-            nPinned += popc(btw);
+            nPinned += PG_COUNT_TABLES ? (info & 7) : popc(btw);
         } else if (blk & pawns) {
             if (diag) {
                 const u64 cap = pawn_att_up(blk) & (1ULL << s);
@@ -690,7 +699,8 @@ PG_HD u32 count_moves_fused(const Board &b)
             }
         }
     });
-    const u64 chk = (pawn_att_up(myK) & tP) | (PG_TAB(knight[ksq]) & tN) | slChk;
+    const u64 chk = ((PG_COUNT_TABLES ? PG_TAB(pawnUp[ksq]) : pawn_att_up(myK)) & tP) | (PG_TAB(knight[ksq]) & tN) |
+                    slChk;
     u64 cm = ~0ULL, xray = 0;
     if (chk) {
         cm = (chk & (chk - 1)) ? 0 : (chk | PG_TAB(between[ksq][ctz(chk)]));

@@ -114,6 +114,7 @@ void build_tables_once()
     for (int s = 0; s < 64; s++) {
         const u64 b = 1ULL << s;
         t.king[s] = sh_n(b) | sh_s(b) | sh_e(b) | sh_w(b) | sh_ne(b) | sh_nw(b) | sh_se(b) | sh_sw(b);
+        t.pawnUp[s] = pawn_att_up(b);
         t.knight[s] = knight_set_att(b);
         t.rookRays[s] = slow_attacks(s, 0, ROOK_DIRS);
         t.bishopRays[s] = slow_attacks(s, 0, BISHOP_DIRS);
@@ -127,6 +128,7 @@ void build_tables_once()
                 if (!(ray & (1ULL << b))) continue;
                 // squares from a towards b, stopping before b
                 t.between[a][b] = ray_walk(a, dirsAll[d][0], dirsAll[d][1], 1ULL << b, false) & ~(1ULL << b);
+                t.pairInfo[a][b] = (uint8_t)(popc(t.between[a][b]) | ((dirsAll[d][0] && dirsAll[d][1]) ? 8 : 0));
                 u64 back = ray_walk(a, -dirsAll[d][0], -dirsAll[d][1], 0, false);
                 t.line[a][b] = ray | back | (1ULL << a);
             }
