@@ -66,6 +66,12 @@ namespace {
 #ifndef PG_ONE_RUN_SUM
 #define PG_ONE_RUN_SUM 1  // such windows sum their counts with a plain warp reduction
 #endif
+#ifndef PG_MIRRORED_STAGE
+#define PG_MIRRORED_STAGE 1  // parents staged mirrored: children are made in their own frame
+#endif
+#ifndef PG_KNOWN_KINGS
+#define PG_KNOWN_KINGS 1  // (with mirrored staging) the count gets both king squares from the parent
+#endif
 #ifndef PG_TILE_NT
 #define PG_TILE_NT 256
 #endif
@@ -559,6 +565,9 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
     }
     const TileParams &P = DD ? sP : Pin;
     __shared__ u64 sb[6][TILE_MAXP];
+    // king squares in the children's frame: the side to move there (the
+    // parent's opponent) and the parent's mover
+    __shared__ uint8_t skO[PG_KNOWN_KINGS ? TILE_MAXP : 1], skS[PG_KNOWN_KINGS ? TILE_MAXP : 1];
     __shared__ u64 sqEnd[TRACK ? TILE_MAXP : 1];
     __shared__ int sdelta[TRACK ? TILE_MAXP : 1];
     __shared__ u32 sroot[TILE_MAXP];
@@ -596,13 +605,20 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
             if (valid) {
                 qEnd = P.pscan[q + 1];
                 if (TRACK) sqEnd[tid] = qEnd;
-                const Board pb = level_get(P.ppl, P.pstride, q);
+                // mirrored staging: the per-parent flips here replace six
+                // byte swaps per child in make-move
+                const Board lb = level_get(P.ppl, P.pstride, q);
+                const Board pb = PG_MIRRORED_STAGE ? flip_board(lb) : lb;
                 sb[0][tid] = pb.mine;
                 sb[1][tid] = pb.pawns;
                 sb[2][tid] = pb.knights;
                 sb[3][tid] = pb.bq;
                 sb[4][tid] = pb.rq;
                 sb[5][tid] = pb.kings;
+                if (PG_KNOWN_KINGS && PG_MIRRORED_STAGE) {
+                    skO[tid] = (uint8_t)ctz(pb.kings & ~pb.mine);
+                    skS[tid] = (uint8_t)ctz(pb.kings & pb.mine);
+                }
                 sroot[tid] = P.proot ? P.proot[q] : (u32)q;  // no root array: account to the parent itself
             }
             const u64 sBeg = max(P.pscan[p], iBeg);
@@ -637,7 +653,8 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
             // ---- generate the window's moves into the shared item list
             // parents without items (none legal, or answered by the table) generate nothing
             if (valid && qEnd > qBeg && qEnd > sBeg && qBeg < sEnd) {
-                const Board b{sb[0][tid], sb[1][tid], sb[2][tid], sb[3][tid], sb[4][tid], sb[5][tid]};
+                const Board sbt{sb[0][tid], sb[1][tid], sb[2][tid], sb[3][tid], sb[4][tid], sb[5][tid]};
+                const Board b = PG_MIRRORED_STAGE ? flip_board(sbt) : sbt;
                 WindowSink sink{sitems, (int)((long long)qBeg - (long long)sBeg), (u32)(sEnd - sBeg), (u32)tid << 16};
                 gen_moves<SV, PG_MOVER_BITS>(b, sink);  // items carry the mover's planes
                 if ((long long)sink.rel != (long long)qEnd - (long long)sBeg) atomicOr(P.err, DERR_GEN_MISMATCH);
@@ -656,8 +673,15 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
                     pl = (int)((it >> 16) & 0xFFu);
                     if (pl < nP) {
                         const Board b{sb[0][pl], sb[1][pl], sb[2][pl], sb[3][pl], sb[4][pl], sb[5][pl]};
-                        const Board ch = make_child<PG_MOVER_BITS>(b, it);
-                        cnt = count_moves<SV>(ch);
+                        Board ch;
+                        if (PG_KNOWN_KINGS && PG_MIRRORED_STAGE) {
+                            int tk;
+                            ch = make_child_mirrored(b, it, &tk, skS[pl]);
+                            cnt = count_moves_k<SV>(ch, skO[pl], tk);
+                        } else {
+                            ch = PG_MIRRORED_STAGE ? make_child_mirrored(b, it) : make_child<PG_MOVER_BITS>(b, it);
+                            cnt = count_moves<SV>(ch);
+                        }
                         if (MODE == MODE_EXPAND) {
                             const u64 g = sBeg + (u64)j - P.itemBase;
                             level_put(P.cpl, P.cstride, g, ch);

@@ -52,6 +52,11 @@
 #ifndef PG_COUNT_TABLES
 #define PG_COUNT_TABLES 1
 #endif
+// PG_MAKE_TABLES 1: make-move takes the from/to bits and the castling rights
+// a move clears from tables, and tests the moving piece against the from bit.
+#ifndef PG_MAKE_TABLES
+#define PG_MAKE_TABLES 1
+#endif
 // PG_KS_LINE 1: the fused count fills both directions of a line from one
 // propagator chain.
 #ifndef PG_KS_LINE
@@ -154,6 +159,8 @@ struct Tables {
     u32 rookShift[64], bishopShift[64];
     u64 pawnUp[64];         // squares a side-to-move pawn on s attacks (its checkers of a king on s)
     uint8_t pairInfo[64][64];  // squares strictly between (bits 0-2) and 8 when the line is a diagonal
+    u64 bit[64];               // 1 << s
+    uint8_t castleClear[64];   // castling rights lost when a piece leaves or lands on s (rook corners)
 };
 
 // Total entries of the fancy-magic attack table (rook part then bishop part).
@@ -656,15 +663,19 @@ PG_HD void rank_pair(u64 eGen, u64 oGen, u64 os, u64 targets, u64 &attacked, u32
 //    every direction build one propagator chain for both the opponent's
 //    fill and this side's fill; the only square an opaque king hides is the
 //    one behind it on a slider checker's line, which is added back (x-ray).
+//
+// ksqIn / tksqIn: the squares of this side's and the opponent's king when the
+// caller knows them (the tile kernel does: they follow from the parent), or
+// negative to find them here.
 template <int SV>
-PG_HD u32 count_moves_fused(const Board &b)
+PG_HD u32 count_moves_fused(const Board &b, int ksqIn = -1, int tksqIn = -1)
 {
     constexpr int M = SvTraits<SV>::shift;
     const u64 pawns = b.pawns & RANKS2TO7;
     const u64 occ = pawns | b.knights | b.bq | b.rq | b.kings;
     const u64 mine = b.mine, theirs = occ ^ mine, empty = ~occ, notMine = ~mine;
     const u64 myK = b.kings & mine;
-    const int ksq = ctz(myK);
+    const int ksq = ksqIn >= 0 ? ksqIn : ctz(myK);
     const u64 tP = pawns & theirs, tN = b.knights & theirs, tB = b.bq & theirs, tR = b.rq & theirs;
     const u32 st = (u32)(b.pawns & 0xFF);
 
@@ -755,7 +766,7 @@ PG_HD u32 count_moves_fused(const Board &b)
         ks_pair<9, false, M>(tB, B, empty, ~FILEH, targets, attacked, n);
 #endif
     }
-    attacked |= pawn_att_down(tP) | knight_set_att(tN) | PG_TAB(king[ctz(b.kings & theirs)]);
+    attacked |= pawn_att_down(tP) | knight_set_att(tN) | PG_TAB(king[tksqIn >= 0 ? tksqIn : ctz(b.kings & theirs)]);
 
     // king
     n += popc(PG_TAB(king[ksq]) & notMine & ~(attacked | xray));
@@ -810,6 +821,18 @@ PG_HD u32 count_moves_fused(const Board &b)
         n += knight_set_count(N, targets);
     }
     return n;
+}
+
+template <int SV>
+PG_HD u32 count_moves(const Board &b);
+
+// count_moves with the two king squares supplied (Kogge-Stone variants; the
+// magic variant finds them itself).
+template <int SV>
+PG_HD u32 count_moves_k(const Board &b, int ksq, int tksq)
+{
+    if (SvTraits<SV>::kogge && PG_FUSED_COUNT) return count_moves_fused<SV>(b, ksq, tksq);
+    return count_moves<SV>(b);
 }
 
 // Legal move count of the side to move (countMoves).
@@ -1053,16 +1076,21 @@ PG_HD Board make_child(const Board &b, u32 mv)
 {
     const int from = mv & 63, to = (mv >> 6) & 63;
     const u32 fl = (mv >> 12) & 15;
-    const u64 src = 1ULL << from, dst = 1ULL << to, sd = src | dst;
+    const u64 src = PG_MAKE_TABLES ? PG_TAB(bit[from]) : 1ULL << from;
+    const u64 dst = PG_MAKE_TABLES ? PG_TAB(bit[to]) : 1ULL << to;
+    const u64 sd = src | dst;
     const u64 st = b.pawns & 0xFF;
     const u64 pawns0 = b.pawns & RANKS2TO7;
     const u64 theirPawns = pawns0 & ~b.mine;
 
-    const u64 mP = MOVER ? maskIf(mv & MV_P) : maskIf((pawns0 >> from) & 1);
-    const u64 mN = MOVER ? maskIf(mv & MV_N) : maskIf((b.knights >> from) & 1);
-    const u64 mB = MOVER ? maskIf(mv & MV_BQ) : maskIf((b.bq >> from) & 1);
-    const u64 mR = MOVER ? maskIf(mv & MV_RQ) : maskIf((b.rq >> from) & 1);
-    const u64 mK = MOVER ? maskIf(mv & MV_K) : maskIf((b.kings >> from) & 1);
+    auto on = [&](u64 plane) -> u64 {  // all ones when the moving piece is on `plane`
+        return PG_MAKE_TABLES ? maskIf((plane & src) != 0) : maskIf((plane >> from) & 1);
+    };
+    const u64 mP = MOVER ? maskIf(mv & MV_P) : on(pawns0);
+    const u64 mN = MOVER ? maskIf(mv & MV_N) : on(b.knights);
+    const u64 mB = MOVER ? maskIf(mv & MV_BQ) : on(b.bq);
+    const u64 mR = MOVER ? maskIf(mv & MV_RQ) : on(b.rq);
+    const u64 mK = MOVER ? maskIf(mv & MV_K) : on(b.kings);
 
     u64 pawns = pawns0 & ~sd;
     u64 kn = b.knights & ~sd;
@@ -1086,7 +1114,9 @@ PG_HD Board make_child(const Board &b, u32 mv)
     const u64 mine = ((b.mine & ~src) | dst) ^ rookHop;
 
     // castling rights: king move, or anything leaving/landing on a rook corner
-    u64 clear = (mK & 3) | ((sd >> 7) & 1) | ((sd & 1) << 1) | ((sd >> 61) & 4) | ((sd >> 53) & 8);
+    u64 clear = PG_MAKE_TABLES
+                    ? (mK & 3) | PG_TAB(castleClear[from]) | PG_TAB(castleClear[to])
+                    : (mK & 3) | ((sd >> 7) & 1) | ((sd & 1) << 1) | ((sd >> 61) & 4) | ((sd >> 53) & 8);
     const u64 st2 = st & ~clear;
 
     // exact en-passant flagging: only when an enemy pawn stands beside dst
@@ -1101,6 +1131,79 @@ PG_HD Board make_child(const Board &b, u32 mv)
     c.bq = flipv(bq);
     c.rq = flipv(rq);
     c.kings = flipv(kings);
+    return c;
+}
+
+// The vertical mirror of every plane of a board (the parent in its child's
+// frame).  The pawn plane's state byte moves to bits 56-63 and the side bit
+// to bit 7, squares no pawn occupies.
+PG_HD Board flip_board(const Board &b)
+{
+    return Board{flipv(b.mine), flipv(b.pawns), flipv(b.knights), flipv(b.bq), flipv(b.rq), flipv(b.kings)};
+}
+
+// make_child on the parent given mirrored (f = flip_board(parent)): the move
+// is applied in the child's own frame, so the child needs no mirroring.
+// Same result as make_child(flip_board(f), mv).  The move's squares are the
+// parent's; in this frame they sit at square ^ 56, the parent's state byte
+// at bits 56-63 and its side bit at bit 7.
+PG_HD Board make_child_mirrored(const Board &f, u32 mv, int *moverKing = nullptr, int stillKing = 0)
+{
+    const int from = mv & 63, to = (mv >> 6) & 63;
+    const u32 fl = (mv >> 12) & 15;
+    const u64 src = PG_TAB(bit[from ^ 56]), dst = PG_TAB(bit[to ^ 56]);
+    const u64 sd = src | dst;
+    const u64 st = f.pawns >> 56;
+    const u64 pawns0 = f.pawns & RANKS2TO7;
+    const u64 theirPawns = pawns0 & ~f.mine;
+
+    const u64 mP = maskIf((pawns0 & src) != 0);
+    const u64 mN = maskIf((f.knights & src) != 0);
+    const u64 mB = maskIf((f.bq & src) != 0);
+    const u64 mR = maskIf((f.rq & src) != 0);
+    const u64 mK = maskIf((f.kings & src) != 0);
+
+    u64 pawns = pawns0 & ~sd;
+    u64 kn = f.knights & ~sd;
+    u64 bq = f.bq & ~sd;
+    u64 rq = f.rq & ~sd;
+    u64 kings = f.kings & ~src;
+
+    const u64 mPromo = maskIf(fl & 8);
+    const u32 pt = fl & 3;  // promotion piece: 0 N, 1 B, 2 R, 3 Q
+    pawns |= dst & mP & ~mPromo;
+    kn |= dst & ((mN & ~mPromo) | (mPromo & maskIf(pt == 0)));
+    bq |= dst & ((mB & ~mPromo) | (mPromo & maskIf(pt == 1 || pt == 3)));
+    rq |= dst & ((mR & ~mPromo) | (mPromo & maskIf(pt >= 2)));
+    kings |= dst & mK;
+
+    // en passant removes the pawn behind the target square (north of it here)
+    pawns &= ~(sh_n(dst) & maskIf(fl == MF_EP));
+    // castling moves the rook: h1->f1 or a1->d1 of the parent, on rank 8 here
+    const u64 rookHop = (fl == MF_KING_CASTLE) ? (0xA0ULL << 56) : (fl == MF_QUEEN_CASTLE ? (0x09ULL << 56) : 0ULL);
+    rq ^= rookHop;
+    const u64 mine = ((f.mine & ~src) | dst) ^ rookHop;
+
+    // castling rights: king move, or anything leaving/landing on a rook corner
+    const u64 clear = (mK & 3) | PG_TAB(castleClear[from]) | PG_TAB(castleClear[to]);
+    const u64 st2 = st & ~clear;
+
+    // exact en-passant flagging: only when an enemy pawn stands beside dst
+    u64 epf = 0;
+    if (fl == MF_DOUBLE_PUSH && ((sh_e(dst) | sh_w(dst)) & theirPawns)) epf = (u64)((from & 7) + 1);
+
+    // the moving side's king square in the child's frame, when asked: where a
+    // king move lands, else `stillKing` (its square before the move)
+    if (moverKing) *moverKing = mK ? (to ^ 56) : stillKing;
+
+    const u64 occ = pawns | kn | bq | rq | kings;
+    Board c;
+    c.mine = occ & ~mine;
+    c.pawns = pawns | ((st2 >> 2) & 3) | ((st2 & 3) << 2) | (epf << 4) | ((~f.pawns & 0x80ULL) << 56);
+    c.knights = kn;
+    c.bq = bq;
+    c.rq = rq;
+    c.kings = kings;
     return c;
 }
 

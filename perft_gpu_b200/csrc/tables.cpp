@@ -115,6 +115,10 @@ void build_tables_once()
         const u64 b = 1ULL << s;
         t.king[s] = sh_n(b) | sh_s(b) | sh_e(b) | sh_w(b) | sh_ne(b) | sh_nw(b) | sh_se(b) | sh_sw(b);
         t.pawnUp[s] = pawn_att_up(b);
+        t.bit[s] = b;
+        // rights of the side to move: 1 king side (rook h1), 2 queen side (a1);
+        // of the opponent: 4 king side (h8), 8 queen side (a8)
+        t.castleClear[s] = (uint8_t)(s == 7 ? 1 : s == 0 ? 2 : s == 63 ? 4 : s == 56 ? 8 : 0);
         t.knight[s] = knight_set_att(b);
         t.rookRays[s] = slow_attacks(s, 0, ROOK_DIRS);
         t.bishopRays[s] = slow_attacks(s, 0, BISHOP_DIRS);

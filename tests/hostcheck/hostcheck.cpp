@@ -92,6 +92,43 @@ uint32_t hc_children_mover(const uint64_t pos[6], int sv, uint64_t *out, uint16_
     return s.n;
 }
 
+// Children made from the mirrored parent (make_child_mirrored), as the tile
+// kernel makes them; the caller compares them with hc_children.
+uint32_t hc_children_mirrored(const uint64_t pos[6], uint64_t *out)
+{
+    const Board b = from_pos48(pos);
+    u32 moves[256];
+    VecSink s{moves, 0};
+    gen_moves<SV_KOGGE>(b, s);
+    const Board f = flip_board(b);
+    for (u32 i = 0; i < s.n; i++) to_pos48(make_child_mirrored(f, moves[i] | (0x5Au << 16)), out + 6 * i);
+    return s.n;
+}
+
+// Move counts of the children made from the mirrored parent with the king
+// squares handed to the count (as the tile kernel does), next to the plain
+// count of the same children; returns the number of mismatches.
+uint32_t hc_counts_known_kings(const uint64_t pos[6], int sv)
+{
+    const Board b = from_pos48(pos);
+    u32 moves[256];
+    VecSink s{moves, 0};
+    gen_moves<SV_KOGGE>(b, s);
+    const Board f = flip_board(b);
+    const int oKing = ctz(f.kings & ~f.mine), sKing = ctz(f.kings & f.mine);
+    uint32_t bad = 0;
+    for (u32 i = 0; i < s.n; i++) {
+        int tk = -1;
+        const Board c = make_child_mirrored(f, moves[i], &tk, sKing);
+        const uint32_t want = with_sv(sv, [&]<int SV>() { return count_moves<SV>(c); });
+        const uint32_t got = with_sv(sv, [&]<int SV>() {
+            return SvTraits<SV>::kogge ? count_moves_fused<SV>(c, oKing, tk) : count_moves<SV>(c);
+        });
+        bad += got != want;
+    }
+    return bad;
+}
+
 uint64_t hc_perft(const uint64_t pos[6], uint32_t depth, int sv)
 {
     const Board b = from_pos48(pos);

@@ -116,3 +116,48 @@ def test_mover_bits_children(hc, golden, sv):
             if n == 0:
                 break
             p = np.array(kids[rng.randrange(n)], dtype=np.uint64)
+
+
+def test_mirrored_make_equals_make(hc, golden):
+    """Children made from the mirrored parent (the tile kernel's make-move)
+    equal make_child's children, in order, on golden positions and seeded
+    walks from them (captures, promotions, castling, en passant included)."""
+    hc.hc_children_mirrored.restype = ctypes.c_uint32
+    rng = random.Random(9)
+    buf = (ctypes.c_uint64 * (6 * 256))()
+    plain = (ctypes.c_uint64 * (6 * 256))()
+    checked = 0
+    for e in golden:
+        p = pos48_from_hex(e["pos48"])
+        for _ in range(16):
+            pp = P6(*[int(x) for x in p])
+            n = hc.hc_children(pp, 0, plain)
+            m = hc.hc_children_mirrored(pp, buf)
+            assert m == n
+            assert list(buf[:6 * n]) == list(plain[:6 * n]), e["name"]
+            checked += n
+            if n == 0:
+                break
+            k = rng.randrange(n)
+            p = np.array(list(plain[6 * k:6 * k + 6]), dtype=np.uint64)
+    assert checked > 5000
+
+
+@pytest.mark.parametrize("sv", SV_ALL, ids=SV_IDS)
+def test_count_with_known_king_squares(hc, golden, sv):
+    """The count with both king squares supplied (from the parent, as the tile
+    kernel supplies them; king moves and castling move one) equals the count
+    that finds them itself, on golden positions and seeded walks."""
+    hc.hc_counts_known_kings.restype = ctypes.c_uint32
+    rng = random.Random(13)
+    buf = (ctypes.c_uint64 * (6 * 256))()
+    for e in golden:
+        p = pos48_from_hex(e["pos48"])
+        for _ in range(12):
+            pp = P6(*[int(x) for x in p])
+            assert hc.hc_counts_known_kings(pp, sv) == 0, e["name"]
+            n = hc.hc_children(pp, 0, buf)
+            if n == 0:
+                break
+            k = rng.randrange(n)
+            p = np.array(list(buf[6 * k:6 * k + 6]), dtype=np.uint64)
