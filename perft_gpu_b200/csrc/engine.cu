@@ -72,6 +72,9 @@ namespace {
 #ifndef PG_KNOWN_KINGS
 #define PG_KNOWN_KINGS 1  // (with mirrored staging) the count gets both king squares from the parent
 #endif
+#ifndef PG_KNOWN_OCC
+#define PG_KNOWN_OCC 1  // (with known kings) and the occupancy and opponent set from make-move
+#endif
 #ifndef PG_TILE_NT
 #define PG_TILE_NT 256
 #endif
@@ -674,7 +677,12 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
                     if (pl < nP) {
                         const Board b{sb[0][pl], sb[1][pl], sb[2][pl], sb[3][pl], sb[4][pl], sb[5][pl]};
                         Board ch;
-                        if (PG_KNOWN_KINGS && PG_MIRRORED_STAGE) {
+                        if (PG_KNOWN_KINGS && PG_MIRRORED_STAGE && PG_KNOWN_OCC) {
+                            int tk;
+                            u64 occ, theirs;
+                            ch = make_child_mirrored(b, it, &tk, skS[pl], &occ, &theirs);
+                            cnt = count_moves_ko<SV>(ch, skO[pl], tk, occ, theirs);
+                        } else if (PG_KNOWN_KINGS && PG_MIRRORED_STAGE) {
                             int tk;
                             ch = make_child_mirrored(b, it, &tk, skS[pl]);
                             cnt = count_moves_k<SV>(ch, skO[pl], tk);

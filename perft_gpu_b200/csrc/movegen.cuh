@@ -667,13 +667,16 @@ PG_HD void rank_pair(u64 eGen, u64 oGen, u64 os, u64 targets, u64 &attacked, u32
 // ksqIn / tksqIn: the squares of this side's and the opponent's king when the
 // caller knows them (the tile kernel does: they follow from the parent), or
 // negative to find them here.
-template <int SV>
-PG_HD u32 count_moves_fused(const Board &b, int ksqIn = -1, int tksqIn = -1)
+//
+// With OCC, occIn / theirsIn are the board's occupancy and the opponent's
+// pieces, which make-move already has.
+template <int SV, bool OCC = false>
+PG_HD u32 count_moves_fused(const Board &b, int ksqIn = -1, int tksqIn = -1, u64 occIn = 0, u64 theirsIn = 0)
 {
     constexpr int M = SvTraits<SV>::shift;
     const u64 pawns = b.pawns & RANKS2TO7;
-    const u64 occ = pawns | b.knights | b.bq | b.rq | b.kings;
-    const u64 mine = b.mine, theirs = occ ^ mine, empty = ~occ, notMine = ~mine;
+    const u64 occ = OCC ? occIn : (pawns | b.knights | b.bq | b.rq | b.kings);
+    const u64 mine = b.mine, theirs = OCC ? theirsIn : occ ^ mine, empty = ~occ, notMine = ~mine;
     const u64 myK = b.kings & mine;
     const int ksq = ksqIn >= 0 ? ksqIn : ctz(myK);
     const u64 tP = pawns & theirs, tN = b.knights & theirs, tB = b.bq & theirs, tR = b.rq & theirs;
@@ -832,6 +835,14 @@ template <int SV>
 PG_HD u32 count_moves_k(const Board &b, int ksq, int tksq)
 {
     if (SvTraits<SV>::kogge && PG_FUSED_COUNT) return count_moves_fused<SV>(b, ksq, tksq);
+    return count_moves<SV>(b);
+}
+
+// count_moves_k with the occupancy and the opponent's pieces supplied too.
+template <int SV>
+PG_HD u32 count_moves_ko(const Board &b, int ksq, int tksq, u64 occ, u64 theirs)
+{
+    if (SvTraits<SV>::kogge && PG_FUSED_COUNT) return count_moves_fused<SV, true>(b, ksq, tksq, occ, theirs);
     return count_moves<SV>(b);
 }
 
@@ -1147,7 +1158,8 @@ PG_HD Board flip_board(const Board &b)
 // Same result as make_child(flip_board(f), mv).  The move's squares are the
 // parent's; in this frame they sit at square ^ 56, the parent's state byte
 // at bits 56-63 and its side bit at bit 7.
-PG_HD Board make_child_mirrored(const Board &f, u32 mv, int *moverKing = nullptr, int stillKing = 0)
+PG_HD Board make_child_mirrored(const Board &f, u32 mv, int *moverKing = nullptr, int stillKing = 0,
+                                u64 *occOut = nullptr, u64 *moverOut = nullptr)
 {
     const int from = mv & 63, to = (mv >> 6) & 63;
     const u32 fl = (mv >> 12) & 15;
@@ -1197,6 +1209,8 @@ PG_HD Board make_child_mirrored(const Board &f, u32 mv, int *moverKing = nullptr
     if (moverKing) *moverKing = mK ? (to ^ 56) : stillKing;
 
     const u64 occ = pawns | kn | bq | rq | kings;
+    if (occOut) *occOut = occ;      // the child's occupancy
+    if (moverOut) *moverOut = mine;  // the moving side's pieces: the child's opponent
     Board c;
     c.mine = occ & ~mine;
     c.pawns = pawns | ((st2 >> 2) & 3) | ((st2 & 3) << 2) | (epf << 4) | ((~f.pawns & 0x80ULL) << 56);

@@ -119,12 +119,14 @@ uint32_t hc_counts_known_kings(const uint64_t pos[6], int sv)
     uint32_t bad = 0;
     for (u32 i = 0; i < s.n; i++) {
         int tk = -1;
-        const Board c = make_child_mirrored(f, moves[i], &tk, sKing);
+        u64 occ = 0, theirs = 0;
+        const Board c = make_child_mirrored(f, moves[i], &tk, sKing, &occ, &theirs);
         const uint32_t want = with_sv(sv, [&]<int SV>() { return count_moves<SV>(c); });
         const uint32_t got = with_sv(sv, [&]<int SV>() {
             return SvTraits<SV>::kogge ? count_moves_fused<SV>(c, oKing, tk) : count_moves<SV>(c);
         });
-        bad += got != want;
+        const uint32_t got2 = with_sv(sv, [&]<int SV>() { return count_moves_ko<SV>(c, oKing, tk, occ, theirs); });
+        bad += (got != want) + (got2 != want);
     }
     return bad;
 }
