@@ -289,10 +289,39 @@ struct LevelDesc {
     int capLog2;  // tile size of this level's items
 };
 
+struct TileParams {
+    const u64 *ppl;   // parent planes, plane i at ppl + i * pstride
+    u64 pstride;
+    const u64 *pscan; // nParents + 1 item offsets
+    const u32 *proot;  // root id of each parent; null: sums go to the parent's own slot
+    u64 nParents;
+    const u32 *tileFirst;  // indexed by absolute tile number
+    u64 itemBase;     // first item of this launch (multiple of the tile size)
+    u64 itemEnd;      // one past the last item
+    int capLog2;      // tile size of this level (the scan's tileFirst granularity)
+    u32 *tileCounter; // work-stealing cursor, zeroed before launch
+    // interior ply outputs (child index = item - itemBase)
+    u64 *cpl;
+    u64 cstride;
+    u32 *ccnt;
+    u32 *croot;
+    // last ply output
+    unsigned long long *rootCounts;
+    u32 *err;
+    // serving: pending-node counter of each query slot (TRACK kernels only)
+    unsigned long long *pending;
+    // device-driven DD_SHARED launches: the plan's entry for this launch
+    const struct TileParams *planEntry;
+};
+
+
 constexpr int DD_MAX_LEVELS = 24;
-// Largest predicted tree (bytes of materialised plies) run as a graph unless
-// PERFT_DD_FORCE=1; PERFT_DD_MAX_GB overrides it.
-constexpr double DD_MAX_BYTES_DEFAULT = 16.0 * (1ull << 30);
+// Largest predicted tree (bytes of materialised plies) run as a graph, on top
+// of the arena check: no limit unless PERFT_DD_MAX_GB sets one.
+constexpr double DD_MAX_BYTES_DEFAULT = 1e30;
+// Plies predicted to have fewer items than this read their launch
+// parameters through shared memory instead of a constant-bank copy node.
+constexpr double DD_CONST_MIN_ITEMS = double(1u << 22);
 struct DevPlan {
     char *base;
     u64 cap;
@@ -304,7 +333,18 @@ struct DevPlan {
     u32 joinN[DD_MAX_LEVELS];
     const u32 *joinIds[DD_MAX_LEVELS];
     int capMax[DD_MAX_LEVELS];  // largest tile (log2 items) for the items of level k
+    // the tile launch of level k's items, completed on the device by the scan
+    // (level pointers and sizes) and copied into c_ddTile before that launch
+    TileParams tp[DD_MAX_LEVELS];
 };
+
+// The parameters of the device-driven tile launch about to run.  A graph
+// copies the plan's entry for the level here (a device-to-device copy node)
+// before each tile launch, so the kernel reads them from the constant bank,
+// as a plain launch reads its parameters, instead of holding plan pointers
+// in registers or shared memory.  Only the device-driven graphs use it, and
+// they run one at a time on the engine's stream.
+__constant__ TileParams c_ddTile;
 
 __device__ __forceinline__ void *dd_take(DevPlan *plan, u64 bytes)
 {
@@ -406,6 +446,16 @@ __device__ void dd_plan_level(DevPlan *plan, int lv, int last, u64 total)
     int cap = plan->capMax[lv] ? plan->capMax[lv] : TILE_CAP_LOG2;
     while (cap > TILE_MIN_LOG2 && (total >> cap) < plan->tileTarget) cap--;
     L.capLog2 = cap;
+    TileParams &T = plan->tp[lv];  // host fields (cursor, outputs, error word) come from the template
+    T.ppl = L.planes;
+    T.pstride = L.stride;
+    T.pscan = L.pscan;
+    T.proot = L.root;
+    T.nParents = L.n;
+    T.tileFirst = L.tileFirst;
+    T.itemBase = 0;
+    T.itemEnd = L.total;
+    T.capLog2 = cap;
     if (last) return;
     LevelDesc &C = plan->lv[lv + 1];
     const u64 m = L.total + plan->joinN[lv + 1];
@@ -423,6 +473,11 @@ __device__ void dd_plan_level(DevPlan *plan, int lv, int last, u64 total)
         C.n = 0;
         L.total = 0;  // nothing is expanded into a level that does not exist
     }
+    T.itemEnd = L.total;
+    T.cpl = C.planes;
+    T.cstride = C.stride;
+    T.ccnt = C.cnt;
+    T.croot = C.root;
 }
 
 __global__ void __launch_bounds__(SCAN_NT) k_dd_scan_apply(DevPlan *plan, int lv)
@@ -484,32 +539,7 @@ __global__ void k_dd_join(DevPlan *plan, int lv, const u64 *__restrict__ pos48, 
 }
 
 // ------------------------------------------------------------ tile kernel
-struct TileParams {
-    const u64 *ppl;   // parent planes, plane i at ppl + i * pstride
-    u64 pstride;
-    const u64 *pscan; // nParents + 1 item offsets
-    const u32 *proot;  // root id of each parent; null: sums go to the parent's own slot
-    u64 nParents;
-    const u32 *tileFirst;  // indexed by absolute tile number
-    u64 itemBase;     // first item of this launch (multiple of the tile size)
-    u64 itemEnd;      // one past the last item
-    int capLog2;      // tile size of this level (the scan's tileFirst granularity)
-    u32 *tileCounter; // work-stealing cursor, zeroed before launch
-    // interior ply outputs (child index = item - itemBase)
-    u64 *cpl;
-    u64 cstride;
-    u32 *ccnt;
-    u32 *croot;
-    // last ply output
-    unsigned long long *rootCounts;
-    u32 *err;
-    // serving: pending-node counter of each query slot (TRACK kernels only)
-    unsigned long long *pending;
-    // device-driven runs (DD kernels only): parent/child level descriptors
-    // written on the device by the previous scan; they override the fields above
-    const struct LevelDesc *dpar;
-    const struct LevelDesc *dch;
-};
+
 
 
 // Emits a parent's moves, keeping only those whose global item index falls
@@ -533,40 +563,29 @@ struct WindowSink {
 // change of its query's pending-node counter: +1 per child written, -1 when
 // a parent's last item is processed.  The counter reaching zero means the
 // query's subtree is fully counted.
-template <int MODE, int SV, bool TRACK = false, bool DD = false>
+// DD: 0 for plain launches (parameters in the parameter bank); DD_SHARED or
+// DD_CONST for the device-driven graph's launches (below).
+enum { DD_NONE = 0, DD_SHARED = 1, DD_CONST = 2 };
+template <int MODE, int SV, bool TRACK = false, int DD = DD_NONE>
 __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pin)
 {
-    // Device-driven runs take the level pointers and sizes from the plan.
-    // They are kept in shared memory, not in registers: held in registers
-    // across the make-and-count loop they cost the count registers (the
-    // kernel runs at the 80-register cap), which measured 5% slower.  Plain
-    // launches read them from the parameter bank.
+    // Device-driven launches take the level pointers and sizes from the plan:
+    //  * DD_CONST reads them from the constant bank (c_ddTile, which the graph
+    //    fills by a copy node before the launch), exactly as a plain launch
+    //    reads its parameter bank.  Used for large plies: held in registers
+    //    across the make-and-count loop the pointers compete with the count at
+    //    the 80-register cap (5% slower), and read from shared memory they
+    //    still cost 1.3%; from the constant bank the count-only launch of the
+    //    4096-position batch takes the same time as a plain launch.
+    //  * DD_SHARED reads the plan entry into shared memory at the start of the
+    //    launch.  Used for small plies, where the copy node's few microseconds
+    //    would cost more than they save.
     __shared__ TileParams sP;
-    if (DD) {
-        if (threadIdx.x == 0) {
-            TileParams q = Pin;
-            const LevelDesc &a = *Pin.dpar;
-            q.ppl = a.planes;
-            q.pstride = a.stride;
-            q.pscan = a.pscan;
-            q.proot = a.root;
-            q.nParents = a.n;
-            q.tileFirst = a.tileFirst;
-            q.itemBase = 0;
-            q.itemEnd = a.total;
-            q.capLog2 = a.capLog2;
-            if (MODE == MODE_EXPAND) {
-                const LevelDesc &c = *Pin.dch;
-                q.cpl = c.planes;
-                q.cstride = c.stride;
-                q.ccnt = c.cnt;
-                q.croot = c.root;
-            }
-            sP = q;
-        }
+    if (DD == DD_SHARED) {
+        if (threadIdx.x == 0) sP = *Pin.planEntry;
         __syncthreads();
     }
-    const TileParams &P = DD ? sP : Pin;
+    const TileParams &P = DD == DD_CONST ? c_ddTile : (DD == DD_SHARED ? sP : Pin);
     __shared__ u64 sb[6][TILE_MAXP];
     // king squares in the children's frame: the side to move there (the
     // parent's opponent) and the parent's mover
@@ -1120,6 +1139,7 @@ private:
         bool overflowed = false;  // the plan did not fit: later calls go host-driven at once
         cudaEvent_t evLeaf0 = nullptr, evLeaf1 = nullptr;  // recorded around the count-only ply
         std::vector<double> predLv;  // predicted nodes per level (empty: no prediction)
+        u64 otherLaunches = 0;       // root, scan and join kernels per replay
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         DevPlan *hTemplate = nullptr;  // pinned
@@ -1177,6 +1197,19 @@ void launch_tile_variant(int sv, int grid, cudaStream_t st, const TileParams &P)
     case SV_HYBRID: k_tile<MODE, SV_HYBRID><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P); break;
     default: k_tile<MODE, SV_KOGGE><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P); break;
     }
+}
+
+// A device-driven tile launch: the two graph variants (Kogge-Stone, split
+// shifts) x the two parameter modes (constant bank for large plies, shared
+// memory for small ones).
+template <int MODE>
+void launch_dd_tile(int sv, bool constParams, int grid, cudaStream_t st, const TileParams &P)
+{
+    const bool split = sv == SV_KOGGE_SPLIT;
+    if (constParams && split) k_tile<MODE, SV_KOGGE_SPLIT, false, DD_CONST><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P);
+    else if (constParams) k_tile<MODE, SV_KOGGE, false, DD_CONST><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P);
+    else if (split) k_tile<MODE, SV_KOGGE_SPLIT, false, DD_SHARED><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P);
+    else k_tile<MODE, SV_KOGGE, false, DD_SHARED><<<grid, TILE_NT, TILE_DYN_SMEM, st>>>(P);
 }
 
 const char *slider_name(int sv)
@@ -1270,10 +1303,14 @@ int Engine::init(const perft_config &cfg)
     gridTile[MODE_EXPAND][SV_HYBRID] = occupancy_grid<MODE_EXPAND, SV_HYBRID>(nsm);
     gridTile[MODE_LEAF][SV_HYBRID] = occupancy_grid<MODE_LEAF, SV_HYBRID>(nsm);
 
-    for (auto fn : {(const void *)k_tile<MODE_LEAF, SV_KOGGE, false, true>,
-                    (const void *)k_tile<MODE_LEAF, SV_KOGGE_SPLIT, false, true>,
-                    (const void *)k_tile<MODE_EXPAND, SV_KOGGE, false, true>,
-                    (const void *)k_tile<MODE_EXPAND, SV_KOGGE_SPLIT, false, true>})
+    for (auto fn : {(const void *)k_tile<MODE_LEAF, SV_KOGGE, false, DD_CONST>,
+                    (const void *)k_tile<MODE_LEAF, SV_KOGGE_SPLIT, false, DD_CONST>,
+                    (const void *)k_tile<MODE_EXPAND, SV_KOGGE, false, DD_CONST>,
+                    (const void *)k_tile<MODE_EXPAND, SV_KOGGE_SPLIT, false, DD_CONST>,
+                    (const void *)k_tile<MODE_LEAF, SV_KOGGE, false, DD_SHARED>,
+                    (const void *)k_tile<MODE_LEAF, SV_KOGGE_SPLIT, false, DD_SHARED>,
+                    (const void *)k_tile<MODE_EXPAND, SV_KOGGE, false, DD_SHARED>,
+                    (const void *)k_tile<MODE_EXPAND, SV_KOGGE_SPLIT, false, DD_SHARED>})
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_DYN_SMEM);
     ddGridScan = 4 * nsm;
     ddEnabled = !(getenv("PERFT_NO_GRAPHS") && getenv("PERFT_NO_GRAPHS")[0] == '1');
@@ -1838,6 +1875,10 @@ int Engine::build_dd(DDGraph &G)
         lvSv[lv] = c.sv;
         lvGrid[lv] = grid_for(mode, c);
         G.hTemplate->capMax[lv] = c.cap;
+        TileParams &T = G.hTemplate->tp[lv];  // the scan fills the level fields on the device
+        T.tileCounter = dCounter;
+        T.rootCounts = (unsigned long long *)G.dOut;
+        T.err = dErr;
         // A ply predicted to have few tiles gets a grid of four CTAs per
         // predicted tile (at least 8) instead of one CTA per resident slot:
         // the tile kernel is persistent, so any grid is correct, and the
@@ -1855,6 +1896,7 @@ int Engine::build_dd(DDGraph &G)
     cudaMemcpyAsync(dIds, G.hIds, 4 * n, cudaMemcpyHostToDevice, stream);
     cudaMemsetAsync(G.dOut, 0, 8 * n, stream);
     cudaMemsetAsync(dErr, 0, 4, stream);
+    G.otherLaunches = (nAt[0] ? 1 : 0) + (nAt[1] ? 1 : 0) + (d >= 2 ? 1 : 0);
     for (int dd = 0; dd <= 1; dd++)
         if (nAt[dd])
             k_init_roots<<<(nAt[dd] + 127) / 128, 128, 0, stream>>>(G.dPos, dIds + offAt[dd], nAt[dd], sPlanes,
@@ -1869,33 +1911,40 @@ int Engine::build_dd(DDGraph &G)
         // levels predicted small take one single-block scan launch instead of three
         if ((int)G.predLv.size() > lv && G.predLv[lv] <= 32768.0) {
             k_dd_scan_small<<<1, 1024, 0, stream>>>(dPlan, lv, last);
+            G.otherLaunches += 1;
         } else {
             k_dd_scan_reduce<<<ddGridScan, SCAN_NT, 0, stream>>>(dPlan, lv);
+            G.otherLaunches += 3;
             k_dd_scan_top<<<1, SCAN_TOP_NT, 0, stream>>>(dPlan, lv, last);
             k_dd_scan_apply<<<ddGridScan, SCAN_NT, 0, stream>>>(dPlan, lv);
         }
         cudaMemsetAsync(dCounter, 0, 4, stream);
+        // Large plies read their launch parameters (completed by the scan)
+        // from the constant bank, copied there by a copy node; small ones
+        // from the plan, through shared memory (no copy node).
+        const bool big = !((int)G.predLv.size() > lv + 1 &&
+                           (last ? G.predLv[lv] * 32.0 : G.predLv[lv + 1]) < DD_CONST_MIN_ITEMS);
+        if (big)
+            cudaMemcpyToSymbolAsync(c_ddTile, &dPlan->tp[lv], sizeof(TileParams), 0, cudaMemcpyDeviceToDevice,
+                                    stream);
         TileParams P;
         memset(&P, 0, sizeof P);
-        P.dpar = &dPlan->lv[lv];
-        P.dch = last ? nullptr : &dPlan->lv[lv + 1];
-        P.tileCounter = dCounter;
-        P.rootCounts = (unsigned long long *)G.dOut;
-        P.err = dErr;
+        P.planEntry = &dPlan->tp[lv];
         const int sv = lvSv[lv];
         const int grid = lvGrid[lv];
         if (last) {
             // external records: event record nodes in the graph (a plain
             // record during capture only orders the capture)
             cudaEventRecordWithFlags(G.evLeaf0, stream, cudaEventRecordExternal);
-            if (sv == SV_KOGGE_SPLIT) k_tile<MODE_LEAF, SV_KOGGE_SPLIT, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
-            else k_tile<MODE_LEAF, SV_KOGGE, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
+            launch_dd_tile<MODE_LEAF>(sv, big, grid, stream, P);
             cudaEventRecordWithFlags(G.evLeaf1, stream, cudaEventRecordExternal);
         } else {
-            if (sv == SV_KOGGE_SPLIT) k_tile<MODE_EXPAND, SV_KOGGE_SPLIT, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
-            else k_tile<MODE_EXPAND, SV_KOGGE, false, true><<<grid, TILE_NT, TILE_DYN_SMEM, stream>>>(P);
+            launch_dd_tile<MODE_EXPAND>(sv, big, grid, stream, P);
             const u32 nj = G.hTemplate->joinN[lv + 1];
-            if (nj) k_dd_join<<<(nj + 127) / 128, 128, 0, stream>>>(dPlan, lv + 1, G.dPos, dErr);
+            if (nj) {
+                k_dd_join<<<(nj + 127) / 128, 128, 0, stream>>>(dPlan, lv + 1, G.dPos, dErr);
+                G.otherLaunches += 1;
+            }
         }
     }
     cudaMemcpyAsync(&G.hFlags[0], &dPlan->overflow, 4, cudaMemcpyDeviceToHost, stream);
@@ -1962,10 +2011,6 @@ int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, boo
             est += sum * 72.0;
         }
         if (est > 0.85 * (double)arena_free()) return PERFT_OK;
-        // Large trees go host-driven: their few host waits cost nothing next
-        // to the plies, and the plain launches' count-only kernel measured
-        // 1.3% faster than the graph's (4096-position batch: 1726 against
-        // 1749 ms), whose level pointers come from the plan.
         if (est > ddMaxBytes) return PERFT_OK;
     }
     if (!G) {
@@ -2000,7 +2045,7 @@ int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, boo
     G->hFlags[2] = G->hFlags[3] = 0;
     ENG_TRY(cudaGraphLaunch(G->exec, stream));
     ENG_TRY(cudaStreamSynchronize(stream));
-    stats.other_launches += 3 + 3ull * (d > 1 ? d - 1 : 0);
+    stats.other_launches += G->otherLaunches;
     stats.expand_launches += d > 2 ? d - 2 : 0;
     stats.leaf_launches += d >= 2 ? 1 : 0;
     stats.graph_launches += 1;

@@ -58,8 +58,8 @@ def _children(pg, pos):
 
 @pytest.mark.parametrize("graphs", ["1", "0"], ids=["graph", "host_driven"])
 def test_batch4096_every_position_equals_reference(engine, wl, cfg_golden, graphs, monkeypatch):
-    """The whole batch host-driven (the default for a tree this large) and as
-    one captured graph (allowed here up to the whole arena)."""
+    """The whole batch as one captured graph (the default when its predicted
+    levels fit the arena) and host-driven."""
     monkeypatch.setenv("PERFT_NO_GRAPHS", "0" if graphs == "1" else "1")
     monkeypatch.setenv("PERFT_DD_MAX_GB", "1000")
     engine.init(device=0)
