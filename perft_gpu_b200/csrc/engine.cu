@@ -336,6 +336,7 @@ struct DevPlan {
     // the tile launch of level k's items, completed on the device by the scan
     // (level pointers and sizes) and copied into c_ddTile before that launch
     TileParams tp[DD_MAX_LEVELS];
+    u32 *tileCounter;  // the tile launches' work-stealing cursor, reset by each scan
 };
 
 // The parameters of the device-driven tile launch about to run.  A graph
@@ -446,6 +447,7 @@ __device__ void dd_plan_level(DevPlan *plan, int lv, int last, u64 total)
     int cap = plan->capMax[lv] ? plan->capMax[lv] : TILE_CAP_LOG2;
     while (cap > TILE_MIN_LOG2 && (total >> cap) < plan->tileTarget) cap--;
     L.capLog2 = cap;
+    *plan->tileCounter = 0;  // the next launch is this level's tile launch
     TileParams &T = plan->tp[lv];  // host fields (cursor, outputs, error word) come from the template
     T.ppl = L.planes;
     T.pstride = L.stride;
@@ -1859,6 +1861,7 @@ int Engine::build_dd(DDGraph &G)
     G.hTemplate->cap = cap;
     G.hTemplate->bump = bump;
     G.hTemplate->tileTarget = 2 * gridTile[MODE_LEAF][G.svL];
+    G.hTemplate->tileCounter = dCounter;
     G.hTemplate->lv[0] = L0;
     for (int dd = 2; dd < d; dd++) {
         G.hTemplate->joinN[d - dd] = nAt[dd];
@@ -1913,12 +1916,17 @@ int Engine::build_dd(DDGraph &G)
             k_dd_scan_small<<<1, 1024, 0, stream>>>(dPlan, lv, last);
             G.otherLaunches += 1;
         } else {
-            k_dd_scan_reduce<<<ddGridScan, SCAN_NT, 0, stream>>>(dPlan, lv);
+            // grid-stride scans: large predicted levels get up to one block
+            // per chunk (64 per SM at most), like the host-driven scan
+            int sg = ddGridScan;
+            if ((int)G.predLv.size() > lv)
+                sg = (int)std::min<double>(64.0 * nsm, std::max<double>(ddGridScan, G.predLv[lv] / SCAN_CHUNK));
+            k_dd_scan_reduce<<<sg, SCAN_NT, 0, stream>>>(dPlan, lv);
             G.otherLaunches += 3;
             k_dd_scan_top<<<1, SCAN_TOP_NT, 0, stream>>>(dPlan, lv, last);
-            k_dd_scan_apply<<<ddGridScan, SCAN_NT, 0, stream>>>(dPlan, lv);
+            k_dd_scan_apply<<<sg, SCAN_NT, 0, stream>>>(dPlan, lv);
         }
-        cudaMemsetAsync(dCounter, 0, 4, stream);
+        // (the scan reset the tile cursor)
         // Large plies read their launch parameters (completed by the scan)
         // from the constant bank, copied there by a copy node; small ones
         // from the plan, through shared memory (no copy node).
