@@ -141,8 +141,8 @@ typedef struct perft_serve_config {
     uint64_t memory_bytes;   /* budget for resident frontiers (0: 90% of the free arena) */
     uint64_t step_items;     /* items a level may advance per iteration (0: 2^27) */
     uint32_t max_in_flight;  /* admitted queries at once (0: 4096, at most 65536) */
-    int32_t  use_tt;         /* 1 (default): frontier levels two plies above the leaves probe,
-                                de-duplicate and store into the engine's transposition table
+    int32_t  use_tt;         /* 1 (default): frontier levels two and three plies above the leaves
+                                probe, de-duplicate and store into the engine's transposition table
                                 (perft_init with tt_log2_entries > 0), shared by every query
                                 and kept across queries; 0: no table */
 } perft_serve_config;

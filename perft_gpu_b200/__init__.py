@@ -357,7 +357,8 @@ def records(path: str, depth: int, batch: int = 4096) -> int:
 def serve_start(memory_bytes: int = 0, step_items: int = 0, max_in_flight: int = 0, use_tt: bool = True) -> None:
     """Starts the continuous-batching server (after init).  With use_tt and an
     engine table (init with tt_log2_entries), the server's frontier levels two
-    plies above the leaves probe, de-duplicate and store into that table."""
+    and three plies above the leaves probe, de-duplicate and store into that
+    table."""
     cfg = ServeConfig()
     lib().perft_serve_config_default(ctypes.byref(cfg))
     cfg.use_tt = 1 if use_tt else 0

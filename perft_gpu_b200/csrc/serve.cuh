@@ -18,19 +18,26 @@
 // another to finish.  A query's count is the same alone or in the mix: it
 // is a sum of exact per-item counts, only the grouping into launches varies.
 //
-// Transposition table: with an engine table and use_tt, every level two plies
-// above the leaves (remaining depth 2) is hashed and probed before its scan,
-// exactly as the engine's own table levels are (k_tt_probe, k_tt_dedup):
-// table hits take the stored count and generate nothing, and identical nodes
-// of the level are searched once.  The level's last ply then sums per node
-// (not per query), and a finish pass stores each searched node, gives every
-// duplicate its owner's count, and adds every node's count to its query.  The
-// table lives in the engine for the life of the process, so it is shared by
-// all queries and keeps its entries across queries.  Nodes two plies above
-// the leaves carry nearly all of the transpositions' savings: the leaf ply
-// below them is ~97% of the work.
+// Transposition table: with an engine table and use_tt, every level two or
+// three plies above the leaves (remaining depth 2 or 3) is hashed and probed
+// before its scan, exactly as the engine's own table levels are (k_tt_probe,
+// k_tt_dedup): table hits take the stored count and generate nothing, and
+// identical nodes of the level are searched once.  Counts then flow up per
+// node, not per query:
+//   * a remaining-depth-3 level expands without pending-count tracking; each
+//     child level (remaining depth 2) it produces sums its leaf ply per node
+//     and, when done, stores its nodes and adds each node's count into its
+//     parent's sum (the engine's k_tt_finish);
+//   * once a remaining-depth-3 level is fully expanded and all its child
+//     levels are done, it is finished like a remaining-depth-2 level of a
+//     depth-2 query: its searched nodes are stored, duplicates take their
+//     owner's count, and every node's count goes to its query, whose pending
+//     count drops by one per node (k_serve_tt_finish).
+// The table lives in the engine for the life of the process, so it is shared
+// by all queries and keeps its entries across queries.
 #pragma once
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -102,7 +109,7 @@ __global__ void __launch_bounds__(256) k_serve_tt_finish(u64 n, const u64 *__res
         key = slot[i];
     }
     count_stat(&ts->stores, stored);
-    // a count two plies deep is below 218^2 < 2^16, so 32 of them sum in 32 bits
+    // a count three plies deep is below 218^3 < 2^24, so 32 of them sum in 32 bits
     const unsigned peers = __match_any_sync(0xffffffffu, key);
     const unsigned long long sum = __reduce_add_sync(peers, (unsigned)v);
     if (i < n && lane == __ffs(peers) - 1) {
@@ -116,6 +123,11 @@ struct ServeLevel {
     int r = 0;
     bool scanned = false;
     bool tt = false;  // a table level: per-node sums, finished by k_serve_tt_finish
+    // a remaining-depth-2 level expanded from a table level of remaining depth
+    // 3: its root array holds parent indices into that level, its counts go
+    // into the parent's sums (k_tt_finish)
+    struct ServeLevel *parent = nullptr;
+    int outstanding = 0;  // (table levels of remaining depth 3) child levels not yet finished
     std::vector<std::pair<u64, u64>> ttMem;  // its hashes, sums and aliases
     u64 *pscan = nullptr;
     u32 *tileFirst = nullptr;
@@ -154,6 +166,8 @@ private:
     int launch(int mode, ServeLevel &S, u64 lo, u64 hi, DeviceLevel *child);
     int probe_level(ServeLevel &S);
     int finish_level(ServeLevel &S);
+    int retire(ServeLevel *S);
+    std::vector<ServeLevel *> waiting;  // table levels fully expanded, waiting for their child levels
 
     std::thread worker;
     std::mutex mu;
@@ -178,7 +192,7 @@ private:
     std::vector<ServeLevel *> pools[SERVE_MAX_R + 1];
     u64 budget = 0, reserved = 0, stepItems = 0;
     u32 maxInFlight = 0, inFlight = 0, maxSlotUsed = 0;
-    int gridLeaf = 0, gridExpand = 0, gridLeafAcc = 0;
+    int gridLeaf = 0, gridExpand = 0, gridLeafAcc = 0, gridExpandTT = 0;
     bool leafSplit = false;
     // the engine's transposition table, when the server uses it
     ulonglong2 *tt = nullptr;
@@ -293,6 +307,7 @@ int Server::start(const perft_serve_config &cfg, char *block, u64 bytes, int dev
     // table levels' last ply: the engine's per-node-sum leaf kernel
     gridLeafAcc = leafSplit ? occupancy_grid<MODE_LEAF, SV_KOGGE_SPLIT>(prop.multiProcessorCount)
                             : occupancy_grid<MODE_LEAF, SV_KOGGE>(prop.multiProcessorCount);
+    gridExpandTT = occupancy_grid<MODE_EXPAND, SV_KOGGE>(prop.multiProcessorCount);
     bySlot.assign(SERVE_MAX_SLOTS, nullptr);
     freeSlots.clear();
     for (u32 s = SERVE_MAX_SLOTS; s-- > 0;) freeSlots.push_back(s);
@@ -321,6 +336,8 @@ int Server::stop()
         for (ServeLevel *S : pools[r]) delete S;
         pools[r].clear();
     }
+    for (ServeLevel *S : waiting) delete S;
+    waiting.clear();
     for (auto &kv : byTicket) delete kv.second;
     byTicket.clear();
     queue.clear();
@@ -483,9 +500,9 @@ int Server::admit()
     return cudaGetLastError() == cudaSuccess ? PERFT_OK : PERFT_ERR_CUDA;
 }
 
-// Hashes and probes a level two plies above the leaves, and de-duplicates
-// its misses; hits and duplicates get no items.  The level keeps the hashes,
-// per-node sums and aliases until k_serve_tt_finish.
+// Hashes and probes a level two or three plies above the leaves, and
+// de-duplicates its misses; hits and duplicates get no items.  The level
+// keeps the hashes, per-node sums and aliases until it is finished.
 int Server::probe_level(ServeLevel &S)
 {
     const u64 n = S.L.n;
@@ -507,7 +524,7 @@ int Server::probe_level(ServeLevel &S)
     if (cudaMemsetAsync(dkey, 0xFF, 8 * dsize, st) != cudaSuccess ||
         cudaMemsetAsync(downer, 0xFF, 4 * dsize, st) != cudaSuccess)
         return PERFT_ERR_CUDA;
-    k_tt_probe<<<nb, 256, 0, st>>>(S.L.planes, S.L.stride, n, 2, true, ttKeyMask, S.L.cnt, S.L.hash, S.L.hash2,
+    k_tt_probe<<<nb, 256, 0, st>>>(S.L.planes, S.L.stride, n, S.r, true, ttKeyMask, S.L.cnt, S.L.hash, S.L.hash2,
                                    S.L.acc, S.L.alias, tt, ttMask, dkey, downer, dsize - 1, dTTStats);
     k_tt_dedup<<<nb, 256, 0, st>>>(n, S.L.cnt, S.L.alias, downer, S.L.hash2, dTTStats);
     launches += 2;
@@ -519,15 +536,47 @@ int Server::probe_level(ServeLevel &S)
 int Server::finish_level(ServeLevel &S)
 {
     const u64 n = S.L.n;
-    k_serve_tt_finish<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, S.L.hash, S.L.hash2, S.L.acc, S.L.alias,
-                                                                    S.L.root, counts, pending, tt, ttMask, dTTStats);
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    if (S.parent)  // into the parent level's per-node sums
+        k_tt_finish<<<nb, 256, 0, st>>>(n, true, S.L.hash, S.L.hash2, S.L.acc, S.L.alias, S.L.root, S.parent->L.acc,
+                                        tt, ttMask, dTTStats);
+    else           // into the queries' counts
+        k_serve_tt_finish<<<nb, 256, 0, st>>>(n, S.L.hash, S.L.hash2, S.L.acc, S.L.alias, S.L.root, counts,
+                                               pending, tt, ttMask, dTTStats);
     launches++;
     return cudaGetLastError() == cudaSuccess ? PERFT_OK : PERFT_ERR_CUDA;
 }
 
+// A level whose items are all processed: finish it (table levels), free it,
+// and finish a waiting parent whose last child level this was.  A table
+// level of remaining depth 3 with child levels still running waits.
+int Server::retire(ServeLevel *S)
+{
+    if (S->tt && S->outstanding > 0) {
+        waiting.push_back(S);
+        return PERFT_OK;
+    }
+    if (S->tt) {
+        const int rc = finish_level(*S);
+        if (rc != PERFT_OK) return rc;
+    }
+    ServeLevel *parent = S->parent;
+    give_back(S->mem);
+    give_back(S->ttMem);
+    delete S;
+    if (parent && --parent->outstanding == 0 && parent->scanned && parent->next >= parent->total) {
+        auto it = std::find(waiting.begin(), waiting.end(), parent);
+        if (it != waiting.end()) {
+            waiting.erase(it);
+            return retire(parent);
+        }
+    }
+    return PERFT_OK;
+}
+
 int Server::scan_level(ServeLevel &S)
 {
-    if (tt && S.r == 2 && !S.tt) {
+    if (tt && (S.r == 2 || S.r == 3) && !S.tt) {
         const int rc = probe_level(S);
         if (rc != PERFT_OK) return rc;
     }
@@ -592,6 +641,12 @@ int Server::launch(int mode, ServeLevel &S, u64 lo, u64 hi, DeviceLevel *child)
         P.pending = nullptr;
         launch_tile_variant<MODE_LEAF>(leafSplit ? SV_KOGGE_SPLIT : SV_KOGGE,
                                        (int)std::min<u64>(gridLeafAcc, nTiles), st, P);
+    } else if (mode == MODE_EXPAND && S.tt) {
+        // a table level expands without pending tracking; the children's
+        // root entries are parent indices (their counts flow into its sums)
+        P.proot = nullptr;
+        P.pending = nullptr;
+        launch_tile_variant<MODE_EXPAND>(SV_KOGGE, (int)std::min<u64>(gridExpandTT, nTiles), st, P);
     } else if (mode == MODE_LEAF && leafSplit)
         k_tile<MODE_LEAF, SV_KOGGE_SPLIT, true>
             <<<(int)std::min<u64>(gridLeaf, nTiles), TILE_NT, TILE_DYN_SMEM, st>>>(P);
@@ -649,18 +704,17 @@ int Server::advance()
                     }
                     int rc = launch(MODE_EXPAND, *S, lo, hi, &C->L);
                     if (rc != PERFT_OK) return rc;
+                    if (S->tt) {
+                        C->parent = S;
+                        S->outstanding++;
+                    }
                     pools[r - 1].push_back(C);
                 }
                 S->next = hi;
             }
             if (S->next >= S->total) {
-                if (S->tt) {
-                    int rc = finish_level(*S);
-                    if (rc != PERFT_OK) return rc;
-                }
-                give_back(S->mem);
-                give_back(S->ttMem);
-                delete S;
+                const int rc = retire(S);
+                if (rc != PERFT_OK) return rc;
             } else {
                 keep.push_back(S);
             }
@@ -670,7 +724,7 @@ int Server::advance()
     // Levels that cannot get memory wait for others to finish; if nothing at
     // all could run for many iterations the budget is too small for the
     // admitted work: fail loudly instead of spinning.
-    bool pendingWork = false;
+    bool pendingWork = !waiting.empty();
     for (int r = 2; r <= SERVE_MAX_R; r++) pendingWork |= !pools[r].empty();
     idleIterations = (launches == launchesBefore && pendingWork) ? idleIterations + 1 : 0;
     return idleIterations > 200 ? PERFT_ERR_OUT_OF_MEMORY : PERFT_OK;

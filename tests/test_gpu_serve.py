@@ -94,16 +94,21 @@ def tt_server(engine):
     engine.init(device=0, arena_bytes=8 << 30)
 
 
-@pytest.mark.parametrize("step_items", [0, 8192], ids=["default", "tiny_steps"])
-def test_served_with_table_equal_alone_and_oracle(tt_server, oracle, step_items):
+@pytest.mark.parametrize("step_items,memory", [(0, 0), (8192, 0), (1 << 16, 64 << 20)],
+                         ids=["default", "tiny_steps", "tight_memory"])
+def test_served_with_table_equal_alone_and_oracle(tt_server, oracle, step_items, memory):
     """With the table resident in the server: every query equals its count
     alone (engine without a table) and the oracle's; identical queries and
-    transpositions are answered from the table or merged."""
+    transpositions are answered from the table or merged.  Tiny steps split
+    the expansion of a level three plies above the leaves into many child
+    levels, which all add into the same parents' sums; a tight budget admits
+    queries a few at a time, so new levels join while others wait for their
+    child levels."""
     pos, depths = _queries(tt_server, 200, seed=21, max_depth=6)
     pos = np.vstack([pos, pos[:40]])  # repeats: answered from the table
     depths = np.concatenate([depths, depths[:40]])
     want = oracle.perft_batch_mt(pos, depths)
-    tt_server.serve_start(step_items=step_items)
+    tt_server.serve_start(memory_bytes=memory, step_items=step_items)
     tickets = [tt_server.serve_submit(p, int(d)) for p, d in zip(pos, depths)]
     got = [tt_server.serve_wait(t, timeout_s=300)[0] for t in tickets]
     assert got == [int(x) for x in want]
@@ -112,7 +117,7 @@ def test_served_with_table_equal_alone_and_oracle(tt_server, oracle, step_items)
     assert st["tt_probes"] > 0 and st["tt_hits"] > 0 and st["tt_merged"] > 0 and st["tt_stores"] > 0
     tt_server.serve_stop()
     # and the same queries without the table in the server
-    tt_server.serve_start(step_items=step_items, use_tt=False)
+    tt_server.serve_start(memory_bytes=memory, step_items=step_items, use_tt=False)
     tickets = [tt_server.serve_submit(p, int(d)) for p, d in zip(pos, depths)]
     assert [tt_server.serve_wait(t, timeout_s=300)[0] for t in tickets] == got
     assert tt_server.serve_stats()["tt_probes"] == 0
