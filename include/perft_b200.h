@@ -122,9 +122,8 @@ int perft_divide(const perft_pos48 *pos, uint32_t depth, char (*moves)[6], uint6
  * lock, and every call, a failing one included, waits for its stream before
  * it returns: the call is synchronous.  The first call on a device does the
  * set-up (uploads the move tables, looks up the scratch address with that
- * device current); make that first call before any stream capture.  Later
- * calls look the address up again and redo the set-up if the device's
- * context was re-created (cudaDeviceReset). */
+ * device current).  Later calls look the address up again and redo the
+ * set-up if the device's context was re-created (cudaDeviceReset). */
 #define PERFT_NOALLOC_SCRATCH_BYTES (32ull << 20)
 int perft_batch_noalloc(const perft_pos48 *d_pos, const uint8_t *depths, uint32_t n,
                         uint64_t *d_out, void *stream);
