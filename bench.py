@@ -609,7 +609,8 @@ def run_ours(args):
         "leaves_per_step": int(tot), "counts_stable": stable, "counts_vs_reference": parity,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(pos.nbytes),
                 "d2h_bytes_per_step": int(8 * n)},
-        "gpu_launches": int(st["leaf_launches"] + st["expand_launches"] + st["other_launches"]),
+        "gpu_launches": int(st["leaf_launches"] + st["expand_launches"] + st["other_launches"]
+                            + st["small_launches"]),
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),

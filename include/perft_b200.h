@@ -264,6 +264,7 @@ typedef struct perft_stats {
     uint64_t tt_duplicates;      /* same-level transpositions expanded once */
     uint64_t tt_stores;          /* entries written */
     uint64_t graph_launches;     /* batches run as one replayed device-driven graph */
+    uint64_t small_launches;     /* single positions of depth 2..5 counted in one launch */
 } perft_stats;
 
 int perft_get_stats(perft_stats *out);

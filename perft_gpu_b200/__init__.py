@@ -92,6 +92,7 @@ class PerftStats(ctypes.Structure):
         ("tt_duplicates", ctypes.c_uint64),
         ("tt_stores", ctypes.c_uint64),
         ("graph_launches", ctypes.c_uint64),
+        ("small_launches", ctypes.c_uint64),
     ]
 
 

@@ -754,6 +754,251 @@ __global__ void __launch_bounds__(TILE_NT, TILE_MINB) k_tile(const TileParams Pi
     }
 }
 
+// ============================================================ small trees
+// One position of depth 2..5 in one launch, with no level buffers.  The level
+// pipeline spends such a tree's time on per-ply latency: a scan and a tile
+// launch per ply, each a few microseconds on a handful of busy SMs.  Here
+// each CTA takes whole subtrees rooted `depth - r` plies below the position
+// (r = 3, or 2 at depth 2) and counts each one in shared memory:
+//   1. thread 0 generates the subtree root's moves;
+//   2. one thread per move makes the child and counts the child's moves (at
+//      r = 2 these counts are the subtree's perft);
+//   3. a block scan of those counts places the grandchildren, and one thread
+//      per child generates the child's moves into a window of the item list;
+//   4. every thread takes items: make the grandchild, count its moves, sum.
+// Every CTA lists the subtree roots for itself (the position's moves, and at
+// depth 5 its children's moves), so no CTA waits for another; the last CTA
+// to finish sums the per-CTA partial counts.  The move generator, make-move
+// and count are the level pipeline's own functions.
+#ifndef PG_SMALL_NT
+#define PG_SMALL_NT 128
+#endif
+constexpr int SMALL_NT = PG_SMALL_NT;  // threads per CTA: small CTAs put more subtrees in flight
+constexpr int SMALL_MINB = 512 / SMALL_NT;
+constexpr int SMALL_MAX_DEPTH = 5;
+constexpr u32 SMALL_LIST_CAP = 4096;  // subtree roots one CTA can list (depth 5)
+constexpr u32 SMALL_WIN = 2048;       // items per window of a subtree's last ply
+constexpr size_t SMALL_DYN_SMEM = sizeof(u32) * (SMALL_LIST_CAP + SMALL_WIN);
+constexpr int SMALL_MAX_GRID = 1024;
+constexpr u32 SMALL_OVERFLOW = 1u << 8;  // more subtree roots than the list holds: not counted
+
+struct SmallState {
+    unsigned long long partial[SMALL_MAX_GRID];  // per CTA
+    unsigned long long count;                    // the last CTA's sum
+    u32 flags;    // 0, SMALL_OVERFLOW or DERR_BAD_POSITION (written by the last CTA)
+    u32 done;     // CTAs finished; atomicInc wraps it back to 0 for the next launch
+    u32 flagAcc;  // flags raised by any CTA; the last CTA reads and clears it
+};
+
+// Exclusive block sum of one u32 per thread; `total` gets the block's sum.
+template <int NT>
+__device__ __forceinline__ u32 block_excl_sum(u32 v, u32 *sw, u32 &total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    u32 inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) sw[w] = inc;
+    __syncthreads();
+    u32 off = 0, tot = 0;
+#pragma unroll
+    for (int i = 0; i < NT / 32; i++) {
+        off += (i < w) ? sw[i] : 0u;
+        tot += sw[i];
+    }
+    __syncthreads();
+    total = tot;
+    return off + inc - v;
+}
+
+// The kernel's phases: the generator into a window, make-and-count, make.
+// PG_SMALL_NOINLINE 1 calls one out-of-line copy of each instead of inlining
+// them at every call site (a tuning build; it measured no faster).
+#ifndef PG_SMALL_NOINLINE
+#define PG_SMALL_NOINLINE 0
+#endif
+#if PG_SMALL_NOINLINE
+#define PG_SMALL_FN __device__ __noinline__
+#else
+#define PG_SMALL_FN __device__ __forceinline__
+#endif
+// Generates b's moves into items[rel0 ..] (those inside [0, n), tagged);
+// returns rel0 plus the number of moves.  PG_SMALL_GEN_SV: the generator's
+// slider variant here (-1: the generator's default, magic lookups).
+#ifndef PG_SMALL_GEN_SV
+#define PG_SMALL_GEN_SV -1
+#endif
+template <int SV>
+PG_SMALL_FN int small_gen(Board b, u32 *items, int rel0, u32 n, u32 tag)
+{
+    WindowSink sink{items, rel0, n, tag};
+    gen_moves<SV, false, PG_SMALL_GEN_SV>(b, sink);
+    return sink.rel;
+}
+
+template <int SV>
+PG_SMALL_FN u32 small_make_count(Board parent, u32 mv, Board *child)
+{
+    const Board c = make_child<false>(parent, mv);
+    if (child) *child = c;
+    return count_moves<SV>(c);
+}
+
+template <int SV>
+PG_SMALL_FN Board small_make(Board parent, u32 mv)
+{
+    return make_child<false>(parent, mv);
+}
+
+// Exclusive offsets of the counts c[0..n) (n <= MAX_LEGAL_MOVES) into
+// off[0..n); returns their total.  Each thread scans SMALL_PER consecutive
+// entries.
+template <int NT>
+__device__ __forceinline__ u32 small_scan(const u32 *c, u32 *off, u32 n, u32 *sw)
+{
+    constexpr int PER = (MAX_LEGAL_MOVES + NT - 1) / NT;
+    const u32 t0 = threadIdx.x * PER;
+    u32 v = 0;
+#pragma unroll
+    for (int k = 0; k < PER; k++) v += (t0 + k < n) ? c[t0 + k] : 0u;
+    u32 total;
+    u32 base = block_excl_sum<NT>(v, sw, total);
+#pragma unroll
+    for (int k = 0; k < PER; k++)
+        if (t0 + k < n) {
+            off[t0 + k] = base;
+            base += c[t0 + k];
+        }
+    __syncthreads();
+    return total;
+}
+
+// listCap: subtree roots a CTA may list, at most SMALL_LIST_CAP.
+template <int SV>
+__global__ void __launch_bounds__(SMALL_NT, SMALL_MINB) k_small_tree(const u64 *__restrict__ pos48, int depth,
+                                                                     u32 listCap, u64 *__restrict__ out,
+                                                                     SmallState *S)
+{
+    __shared__ Board sB1[MAX_LEGAL_MOVES];  // the position's children (depth 5)
+    __shared__ Board sX[MAX_LEGAL_MOVES];   // the current subtree root's children
+    __shared__ u32 sM1[MAX_LEGAL_MOVES];    // the position's moves
+    __shared__ u32 sMR[MAX_LEGAL_MOVES];    // the current subtree root's moves
+    __shared__ u32 sC[MAX_LEGAL_MOVES];     // children's move counts
+    __shared__ u32 sOff[MAX_LEGAL_MOVES];   // and their exclusive offsets
+    __shared__ u32 swarp[SMALL_NT / 32];
+    __shared__ u32 sN;
+    __shared__ unsigned long long sSum[SMALL_NT / 32];
+    __shared__ bool sLast;
+    extern __shared__ __align__(16) u32 sdyn[];
+    u32 *sList = sdyn;                   // depth 5: subtree roots as (child << 16) | move
+    u32 *sItems = sdyn + SMALL_LIST_CAP;  // grandchildren as (child << 16) | move
+
+    const int tid = threadIdx.x, lane = tid & 31;
+    u64 p[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) p[k] = pos48[k];
+    const Board root = from_pos48(p);
+    const int r = depth >= 3 ? 3 : 2;
+    const int pre = depth - r;  // plies from the position to the subtree roots: 0, 1 or 2
+    u32 flags = validate_pos48(p) != 0 ? DERR_BAD_POSITION : 0u;
+    u32 nRoots = 1;
+    if (!flags && pre >= 1) {
+        if (tid == 0) sN = (u32)small_gen<SV>(root, sM1, 0, MAX_LEGAL_MOVES, 0u);
+        __syncthreads();
+        const u32 n1 = sN;
+        nRoots = n1;
+        if (n1 > (u32)MAX_LEGAL_MOVES) flags = SMALL_OVERFLOW;
+        if (!flags && pre == 2) {
+            for (u32 t = tid; t < n1; t += SMALL_NT) sC[t] = small_make_count<SV>(root, sM1[t], &sB1[t]);
+            __syncthreads();
+            const u32 total = small_scan<SMALL_NT>(sC, sOff, n1, swarp);
+            if (total > listCap) {
+                flags = SMALL_OVERFLOW;
+            } else {
+                for (u32 t = tid; t < n1; t += SMALL_NT)
+                    if (sC[t]) small_gen<SV>(sB1[t], sList, (int)sOff[t], listCap, t << 16);
+                nRoots = total;
+            }
+        }
+        __syncthreads();  // every thread has read sN and the lists before the loop rewrites them
+    }
+
+    unsigned long long acc = 0;
+    for (u32 s = blockIdx.x; !flags && s < nRoots; s += gridDim.x) {
+        Board R = root;
+        if (pre == 1) R = small_make<SV>(root, sM1[s]);
+        if (pre == 2) {
+            const u32 e = sList[s];
+            R = small_make<SV>(sB1[e >> 16], e & 0xFFFFu);
+        }
+        if (tid == 0) sN = (u32)small_gen<SV>(R, sMR, 0, MAX_LEGAL_MOVES, 0u);
+        __syncthreads();
+        const u32 nA = sN;
+        if (nA > (u32)MAX_LEGAL_MOVES) {
+            flags = SMALL_OVERFLOW;
+            break;
+        }
+        for (u32 t = tid; t < nA; t += SMALL_NT) {
+            const u32 c = small_make_count<SV>(R, sMR[t], &sX[t]);
+            sC[t] = c;
+            if (r == 2) acc += c;
+        }
+        __syncthreads();
+        if (r == 2) continue;  // sMR, sC and sN are rewritten only after this barrier
+        const u32 T = small_scan<SMALL_NT>(sC, sOff, nA, swarp);
+        for (u32 w0 = 0; w0 < T; w0 += SMALL_WIN) {
+            const u32 wn = min(SMALL_WIN, T - w0);
+            for (u32 t = tid; t < nA; t += SMALL_NT) {
+                const u32 c = sC[t], off = sOff[t];
+                if (c && off + c > w0 && off < w0 + wn)
+                    small_gen<SV>(sX[t], sItems, (int)((long long)off - (long long)w0), wn, t << 16);
+            }
+            __syncthreads();
+            for (u32 j = tid; j < wn; j += SMALL_NT) {
+                const u32 it = sItems[j];
+                acc += small_make_count<SV>(sX[it >> 16], it & 0xFFFFu, nullptr);
+            }
+            __syncthreads();
+        }
+    }
+
+    // per-CTA sum, then the last CTA to finish adds them up
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) sSum[tid >> 5] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long t = 0;
+#pragma unroll
+        for (int i = 0; i < SMALL_NT / 32; i++) t += sSum[i];
+        S->partial[blockIdx.x] = t;
+        if (flags) atomicOr(&S->flagAcc, flags);
+        __threadfence();
+        sLast = atomicInc(&S->done, gridDim.x - 1) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!sLast) return;
+    __threadfence();
+    unsigned long long t = 0;
+    for (u32 i = tid; i < gridDim.x; i += SMALL_NT) t += __ldcg(&S->partial[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0) sSum[tid >> 5] = t;
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long sum = 0;
+#pragma unroll
+        for (int i = 0; i < SMALL_NT / 32; i++) sum += sSum[i];
+        const u32 all = atomicExch(&S->flagAcc, 0u) | flags;
+        S->count = all ? 0ull : sum;
+        S->flags = all;
+        if (!all) out[0] = sum;
+    }
+}
+
 // ====================================================== transposition table
 // Lockless table of 16-byte entries {verify ^ value, value} at the slot the
 // slot key picks: a torn or foreign entry fails the XOR check (the
@@ -1149,6 +1394,12 @@ private:
         u64 *hFlags = nullptr;         // pinned: overflow, device error, leaf items
     };
     std::vector<DDGraph> ddCache;
+    // one-launch small trees (k_small_tree)
+    SmallState *dSmall = nullptr;
+    int smallGrid = 0;
+    bool smallEnabled = true;
+    u32 smallListCap = SMALL_LIST_CAP;
+    int run_small(const u64 *dPos, int depth, u64 *dOut, u64 *hOut, bool &handled);
     bool ddEnabled = true;
     bool ddForce = false;  // PERFT_DD_FORCE=1: skip the size estimate (tests the overflow fallback)
     double ddMaxBytes = DD_MAX_BYTES_DEFAULT;
@@ -1315,6 +1566,26 @@ int Engine::init(const perft_config &cfg)
                     (const void *)k_tile<MODE_EXPAND, SV_KOGGE_SPLIT, false, DD_SHARED>})
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_DYN_SMEM);
     ddGridScan = 4 * nsm;
+    {
+        ENG_TRY(cudaMalloc(&dSmall, sizeof(SmallState)));
+        ENG_TRY(cudaMemset(dSmall, 0, sizeof(SmallState)));
+        ENG_TRY(cudaFuncSetAttribute(k_small_tree<SV_KOGGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)SMALL_DYN_SMEM));
+        int perSm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_small_tree<SV_KOGGE>, SMALL_NT, SMALL_DYN_SMEM) !=
+                cudaSuccess ||
+            perSm < 1)
+            perSm = 1;
+        smallGrid = std::min(SMALL_MAX_GRID, perSm * nsm);
+        smallEnabled = !(getenv("PERFT_SMALL_TREE") && getenv("PERFT_SMALL_TREE")[0] == '0');
+        // PERFT_SMALL_LIST_CAP=k lists at most k depth-5 subtree roots per CTA:
+        // a test setting that sends ordinary positions down the fallback
+        smallListCap = SMALL_LIST_CAP;
+        if (const char *c = getenv("PERFT_SMALL_LIST_CAP")) {
+            const long v = atol(c);
+            if (v >= 1 && v <= (long)SMALL_LIST_CAP) smallListCap = (u32)v;
+        }
+    }
     ddEnabled = !(getenv("PERFT_NO_GRAPHS") && getenv("PERFT_NO_GRAPHS")[0] == '1');
     ddForce = getenv("PERFT_DD_FORCE") && getenv("PERFT_DD_FORCE")[0] == '1';
     ddMaxBytes = DD_MAX_BYTES_DEFAULT;
@@ -1359,6 +1630,8 @@ void Engine::shutdown()
     dTTStats = nullptr;
     cudaFree(dCounter);
     cudaFree(dErr);
+    if (dSmall) cudaFree(dSmall);
+    dSmall = nullptr;
     cudaFreeHost(hPinned);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
@@ -2075,6 +2348,29 @@ int Engine::run_dd(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, boo
     return PERFT_OK;
 }
 
+// One position of depth 2..5: the whole tree in one k_small_tree launch and
+// one 16-byte read-back (count and flags).  Not handled (the level pipeline
+// runs it) when disabled, outside those depths, or when the position has more
+// depth-5 subtree roots than a CTA can list.  With hOut the count is also
+// returned to the host from the same read-back.
+int Engine::run_small(const u64 *dPos, int depth, u64 *dOut, u64 *hOut, bool &handled)
+{
+    handled = false;
+    if (!smallEnabled || depth < 2 || depth > SMALL_MAX_DEPTH) return PERFT_OK;
+    k_small_tree<SV_KOGGE><<<smallGrid, SMALL_NT, SMALL_DYN_SMEM, stream>>>(dPos, depth, smallListCap, dOut,
+                                                                            dSmall);
+    ENG_TRY(cudaGetLastError());
+    ENG_TRY(cudaMemcpyAsync(hPinned + 4, &dSmall->count, 16, cudaMemcpyDeviceToHost, stream));
+    ENG_TRY(cudaStreamSynchronize(stream));
+    const u32 flags = (u32)hPinned[5];
+    if (flags & DERR_BAD_POSITION) return PERFT_ERR_INVALID_ARG;
+    if (flags) return PERFT_OK;  // too many subtree roots for one CTA's list
+    if (hOut) *hOut = hPinned[4];
+    stats.small_launches += 1;
+    handled = true;
+    return PERFT_OK;
+}
+
 int Engine::run_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *out)
 {
     if (n > ioCap) {
@@ -2090,6 +2386,12 @@ int Engine::run_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *ou
         drop_dd();
     }
     ENG_TRY(cudaMemcpyAsync(ioPos, pos, 48ull * n, cudaMemcpyHostToDevice, stream));
+    if (n == 1) {
+        bool handled = false;
+        ENG_TRY(cudaSetDevice(device));
+        const int rc = run_small(ioPos, depths[0], ioOut, out, handled);
+        if (rc != PERFT_OK || handled) return rc;
+    }
     const int rc = run_batch(ioPos, depths, n, ioOut);
     if (rc != PERFT_OK) return rc;
     ENG_TRY(cudaMemcpyAsync(out, ioOut, 8ull * n, cudaMemcpyDeviceToHost, stream));
@@ -2110,6 +2412,11 @@ int Engine::sync_and_check_errors()
 int Engine::run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut)
 {
     ENG_TRY(cudaSetDevice(device));
+    if (n == 1) {
+        bool handled = false;
+        const int rc = run_small(dPos, depths[0], dOut, nullptr, handled);
+        if (rc != PERFT_OK || handled) return rc;
+    }
     {
         bool handled = false;
         const int rc = run_dd(dPos, depths, n, dOut, handled);

@@ -992,16 +992,17 @@ PG_HD void emit_pawn(Sink &out, int from, int to, u32 flags)
 enum : u32 { MV_P = 1u << 24, MV_N = 2u << 24, MV_BQ = 4u << 24, MV_RQ = 8u << 24, MV_K = 16u << 24 };
 
 // Generates every legal move of the side to move.  Emits exactly
-// count_moves<SV>(b) moves.
-template <int SV, bool MOVER = false, class Sink>
+// count_moves<SV>(b) moves.  GENSV >= 0 forces the slider variant of the
+// per-piece targets and of the opponent's attack map.
+template <int SV, bool MOVER = false, int GENSV = -1, class Sink>
 PG_HD void gen_moves(const Board &b, Sink &out)
 {
     // per-piece targets: one magic lookup per slider beats a single-bit
     // Kogge-Stone fill in every variant; the variant still decides the
     // set-wise opponent attack map
-    constexpr int GEN_SV = PG_GEN_MAGIC ? SV_MAGIC : SV;
+    constexpr int GEN_SV = GENSV >= 0 ? GENSV : (PG_GEN_MAGIC ? SV_MAGIC : SV);
     Ctx c;
-    setup_ctx<PG_GEN_MAGIC_ATTACKS ? GEN_SV : SV>(b, c);
+    setup_ctx<GENSV >= 0 ? GENSV : (PG_GEN_MAGIC_ATTACKS ? GEN_SV : SV)>(b, c);
     const u64 notMine = ~c.mine;
     const u32 mvP = MOVER ? MV_P : 0, mvN = MOVER ? MV_N : 0, mvK = MOVER ? MV_K : 0;
     emit_targets(out, c.ksq | mvK, PG_TAB(king[c.ksq]) & notMine & ~c.attacked);

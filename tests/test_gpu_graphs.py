@@ -37,7 +37,9 @@ def test_graph_path_matches_host_path(engine, golden):
             dd = [engine.perft_batch(pos, d) for d in (2, 3, 4)]
             assert all(np.array_equal(a, b) for a, b in zip(host, dd))
             assert engine.perft(p, 5) == int(start["counts"]["5"])
-        assert engine.stats()["graph_launches"] >= 12
+        st = engine.stats()
+        assert st["graph_launches"] >= 9  # the three batches per pass; perft(5) of one position is one launch
+        assert st["small_launches"] == 3
     finally:
         engine.init(device=0, arena_bytes=8 << 30)
 

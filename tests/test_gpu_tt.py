@@ -35,12 +35,21 @@ def test_tt_matches_golden_cold_and_warm(tt_engine, golden):
     assert st["tt_entries"] == 1 << 22 and st["tt_hits"] > 0
 
 
-def test_tt_single_positions_match_no_tt(tt_engine, oracle):
+@pytest.mark.parametrize("small", ["1", "0"], ids=["small_tree", "table_levels"])
+def test_tt_single_positions_match_no_tt(tt_engine, oracle, small, monkeypatch):
+    """Single positions of depth 2-5 take the one-launch small-tree kernel
+    even with a table; with that kernel off they run the table levels."""
+    monkeypatch.setenv("PERFT_SMALL_TREE", small)
+    tt_engine.init(device=0, arena_bytes=4 << 30, tt_log2_entries=22)
     pos = tt_engine.random_playouts(seed=808, n=40, min_plies=6, max_plies=40)
+    tt_engine.reset_stats()
     for d in (2, 3, 4, 5):
         want = oracle.perft_batch_mt(pos[:8], d)
         got = [tt_engine.perft(p, d) for p in pos[:8]]
         assert got == [int(x) for x in want], d
+    st = tt_engine.stats()
+    assert st["small_launches"] == (32 if small == "1" else 0)
+    assert (st["tt_probes"] > 0) == (small == "0")
     depths = np.array([5] * 40, dtype=np.uint8)
     got = tt_engine.perft_batch(pos, depths)
     assert np.array_equal(got, oracle.perft_batch_mt(pos, 5))
