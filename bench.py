@@ -311,9 +311,10 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ GPU arm
 def single_form_step(pg, d_pos, depths, d_out):
-    """The plain one-position-per-launch form: each position is copied into one
-    fixed device slot and searched by its own perft_batch_device call (a fixed
-    slot lets the engine reuse its per-depth launch graphs)."""
+    """The one-position-per-call form: each position is copied into one fixed
+    device slot and searched by its own perft_batch_device call (a fixed slot
+    lets the engine reuse its per-depth launch graphs; positions of depth 2-5
+    take the one-launch small-tree kernel)."""
     import torch
     n = len(depths)
     slot = torch.zeros(6, dtype=torch.int64, device="cuda")
@@ -402,6 +403,31 @@ def measure_configs(args, pg, device, d_pos, depths, batch_ms_per_step, golden):
         "steps": 1, "ms_per_step": ms, "value": float(single.sum()) / (ms / 1e3), "unit": UNIT,
         "equals_reference": bool(np.array_equal(single, want)) if want is not None else None,
         "batched_over_single": ms / batch_ms_per_step, "clocks": clk}
+
+    # the same again, one position per call through the host-driven level
+    # pipeline: per ply a scan whose total the host reads back, then a tile
+    # launch; no captured graph and no small-tree kernel.  This is the shape of
+    # the reference's one-position driver (a level loop with a device
+    # synchronisation per ply, perft_bb.h:1027-1138).
+    saved = {k: os.environ.get(k) for k in ("PERFT_NO_GRAPHS", "PERFT_SMALL_TREE")}
+    os.environ.update({"PERFT_NO_GRAPHS": "1", "PERFT_SMALL_TREE": "0"})
+    try:
+        pg.init(device=device, arena_bytes=int(args.arena_gb * (1 << 30)))
+        step = single_form_step(pg, d_pos, depths, so)
+        ms2, clk2 = device_timed(step, 1, device)
+        levels = so.cpu().numpy().view(np.uint64)
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    out["batch4096_single_levels"] = {
+        "workload": BATCH_DESC.format(n=n) + ", one perft_batch_device call per position, host-driven level "
+                                             "pipeline (no captured graph, no small-tree kernel)",
+        "steps": 1, "ms_per_step": ms2, "value": float(levels.sum()) / (ms2 / 1e3), "unit": UNIT,
+        "equals_reference": bool(np.array_equal(levels, want)) if want is not None else None,
+        "batched_over_single_levels": ms2 / batch_ms_per_step, "clocks": clk2}
 
     # transposition-table positions at depths 9-10 (2^30 entries), after the
     # depth-8 check without and with the table against the reference

@@ -1080,6 +1080,11 @@ __device__ __forceinline__ void count_stat(unsigned long long *ctr, bool hit)
     if (threadIdx.x == 0 && sCount) atomicAdd(ctr, (unsigned long long)sCount);
 }
 
+// PG_PROBE_OVERLAP 1: the table load overlaps the de-duplication insert.
+#ifndef PG_PROBE_OVERLAP
+#define PG_PROBE_OVERLAP 0
+#endif
+
 // Hash every node, probe the table, and insert misses into the level's
 // de-duplication set (lowest index wins).  Hits get their value and no
 // children; their alias is ALIAS_HIT.  Misses keep the set slot in alias.
@@ -1101,6 +1106,16 @@ __global__ void __launch_bounds__(256) k_tt_probe(const u64 *__restrict__ planes
         hash[i] = h;
         hash2[i] = g;
         acc[i] = 0;
+#if PG_PROBE_OVERLAP
+        // The table load stays in flight while the node joins the
+        // de-duplication set: every node joins, hits included.  Identical
+        // nodes read the same entry (nothing writes the table during a
+        // probe), so a hit never owns a slot that a miss with the same keys
+        // aliases; a miss sharing only the slot key with a hit owner is
+        // searched on its own, like any slot-key collision.
+        const ulonglong2 e = probe ? tt[h & ttMask] : make_ulonglong2(0ull, 1ull);
+        {
+#else
         if (probe) {
             const ulonglong2 e = tt[h & ttMask];
             if ((e.x ^ e.y) == g) {
@@ -1111,6 +1126,7 @@ __global__ void __launch_bounds__(256) k_tt_probe(const u64 *__restrict__ planes
             }
         }
         if (!hit) {
+#endif
             u32 placed = ALIAS_NOSLOT;
             if (h != DEDUP_EMPTY) {
                 u64 slot = (h * 0x9E3779B97F4A7C15ULL >> 17) & dMask;
@@ -1128,6 +1144,14 @@ __global__ void __launch_bounds__(256) k_tt_probe(const u64 *__restrict__ planes
             }
             alias[i] = placed;
         }
+#if PG_PROBE_OVERLAP
+        if (probe && (e.x ^ e.y) == g) {
+            hit = true;
+            acc[i] = e.y;
+            cnt[i] = 0;
+            alias[i] = ALIAS_HIT;
+        }
+#endif
     }
     if (probe) {
         count_stat(&ts->probes, i < n);
@@ -1236,7 +1260,9 @@ class Engine {
 public:
     int init(const perft_config &cfg);
     void shutdown();
-    int run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut);
+    // trySmall: a single position of depth 2..5 tries the one-launch
+    // small-tree kernel first (false when the caller already tried it)
+    int run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, bool trySmall = true);
     // Host buffers: staged through engine-owned device buffers that persist
     // across calls (no per-call allocation; stable addresses let replayed
     // graphs be reused).
@@ -2376,6 +2402,7 @@ int Engine::run_small(const u64 *dPos, int depth, u64 *dOut, u64 *hOut, bool &ha
 
 int Engine::run_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *out)
 {
+    ENG_TRY(cudaSetDevice(device));  // the staging buffers and the stream belong to the engine's device
     if (n > ioCap) {
         if (ioPos) cudaFree(ioPos);
         if (ioOut) cudaFree(ioOut);
@@ -2391,11 +2418,10 @@ int Engine::run_batch_host(const u64 *pos, const uint8_t *depths, u32 n, u64 *ou
     ENG_TRY(cudaMemcpyAsync(ioPos, pos, 48ull * n, cudaMemcpyHostToDevice, stream));
     if (n == 1) {
         bool handled = false;
-        ENG_TRY(cudaSetDevice(device));
         const int rc = run_small(ioPos, depths[0], ioOut, out, handled);
         if (rc != PERFT_OK || handled) return rc;
     }
-    const int rc = run_batch(ioPos, depths, n, ioOut);
+    const int rc = run_batch(ioPos, depths, n, ioOut, false);
     if (rc != PERFT_OK) return rc;
     ENG_TRY(cudaMemcpyAsync(out, ioOut, 8ull * n, cudaMemcpyDeviceToHost, stream));
     ENG_TRY(cudaStreamSynchronize(stream));
@@ -2412,10 +2438,10 @@ int Engine::sync_and_check_errors()
     return PERFT_OK;
 }
 
-int Engine::run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut)
+int Engine::run_batch(const u64 *dPos, const uint8_t *depths, u32 n, u64 *dOut, bool trySmall)
 {
     ENG_TRY(cudaSetDevice(device));
-    if (n == 1) {
+    if (n == 1 && trySmall) {
         bool handled = false;
         const int rc = run_small(dPos, depths[0], dOut, nullptr, handled);
         if (rc != PERFT_OK || handled) return rc;
