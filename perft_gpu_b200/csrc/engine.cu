@@ -1080,11 +1080,6 @@ __device__ __forceinline__ void count_stat(unsigned long long *ctr, bool hit)
     if (threadIdx.x == 0 && sCount) atomicAdd(ctr, (unsigned long long)sCount);
 }
 
-// PG_PROBE_OVERLAP 1: the table load overlaps the de-duplication insert.
-#ifndef PG_PROBE_OVERLAP
-#define PG_PROBE_OVERLAP 0
-#endif
-
 // Hash every node, probe the table, and insert misses into the level's
 // de-duplication set (lowest index wins).  Hits get their value and no
 // children; their alias is ALIAS_HIT.  Misses keep the set slot in alias.
@@ -1106,16 +1101,6 @@ __global__ void __launch_bounds__(256) k_tt_probe(const u64 *__restrict__ planes
         hash[i] = h;
         hash2[i] = g;
         acc[i] = 0;
-#if PG_PROBE_OVERLAP
-        // The table load stays in flight while the node joins the
-        // de-duplication set: every node joins, hits included.  Identical
-        // nodes read the same entry (nothing writes the table during a
-        // probe), so a hit never owns a slot that a miss with the same keys
-        // aliases; a miss sharing only the slot key with a hit owner is
-        // searched on its own, like any slot-key collision.
-        const ulonglong2 e = probe ? tt[h & ttMask] : make_ulonglong2(0ull, 1ull);
-        {
-#else
         if (probe) {
             const ulonglong2 e = tt[h & ttMask];
             if ((e.x ^ e.y) == g) {
@@ -1126,7 +1111,6 @@ __global__ void __launch_bounds__(256) k_tt_probe(const u64 *__restrict__ planes
             }
         }
         if (!hit) {
-#endif
             u32 placed = ALIAS_NOSLOT;
             if (h != DEDUP_EMPTY) {
                 u64 slot = (h * 0x9E3779B97F4A7C15ULL >> 17) & dMask;
@@ -1144,14 +1128,6 @@ __global__ void __launch_bounds__(256) k_tt_probe(const u64 *__restrict__ planes
             }
             alias[i] = placed;
         }
-#if PG_PROBE_OVERLAP
-        if (probe && (e.x ^ e.y) == g) {
-            hit = true;
-            acc[i] = e.y;
-            cnt[i] = 0;
-            alias[i] = ALIAS_HIT;
-        }
-#endif
     }
     if (probe) {
         count_stat(&ts->probes, i < n);
