@@ -278,6 +278,22 @@ PG_HD u64 sh_sw(u64 x) { return (x >> 9) & ~FILEH; }
 // Left:  t = lo * 2^K (wide) gives lo << K and lo >> (32-K); hi' = hi*2^K + that.
 // Right: hi * 2^(32-K) (wide) plus umulhi(lo, 2^(32-K)) = lo >> K gives both
 // words at once (the two parts occupy disjoint bits).  Host builds shift.
+// n + popc(x).  With PG_POPC_IMAD the two half-word counts are added by
+// multiply-adds with the opaque factor c_pow2[0] = 1: the FMA pipe, which the
+// count leaves mostly idle, instead of an IADD3 on the ALU pipe that binds it.
+#ifndef PG_POPC_IMAD
+#define PG_POPC_IMAD 1
+#endif
+PG_HD u32 add_popc(u32 n, u64 x)
+{
+#if defined(__CUDA_ARCH__) && PG_POPC_IMAD
+    const u32 one = c_pow2[0];
+    return (u32)__popc((u32)(x >> 32)) * one + ((u32)__popc((u32)x) * one + n);
+#else
+    return n + popc(x);
+#endif
+}
+
 template <int K>
 PG_HD u64 shl_fma(u64 x)
 {
@@ -600,7 +616,7 @@ PG_HD void ks_line(u64 eGen, u64 oGen, u64 p0, u64 wrapUp, u64 wrapDown, u64 tar
         e |= p2 & shl<4 * S, MODE>(e);
         o |= p2 & shl<4 * S, MODE>(o);
         attacked |= shl<S, MODE>(e) & wrapUp;
-        n += popc(shl<S, MODE>(o) & wrapUp & targets);
+        n = add_popc(n, shl<S, MODE>(o) & wrapUp & targets);
     }
     {
         const u64 q1 = shr<S, MODE>(p1), q2 = shr<3 * S, MODE>(p2);
@@ -612,7 +628,7 @@ PG_HD void ks_line(u64 eGen, u64 oGen, u64 p0, u64 wrapUp, u64 wrapDown, u64 tar
         e |= q2 & shr<4 * S, MODE>(e);
         o |= q2 & shr<4 * S, MODE>(o);
         attacked |= shr<S, MODE>(e) & wrapDown;
-        n += popc(shr<S, MODE>(o) & wrapDown & targets);
+        n = add_popc(n, shr<S, MODE>(o) & wrapDown & targets);
     }
 }
 
@@ -649,10 +665,10 @@ PG_HD void rank_pair(u64 eGen, u64 oGen, u64 os, u64 targets, u64 &attacked, u32
 {
     if (!WEST) {
         attacked |= east_sub(eGen, os);
-        n += popc(east_sub(oGen, os) & targets);
+        n = add_popc(n, east_sub(oGen, os) & targets);
     } else {
         attacked |= brev64(east_sub(brev64(eGen), os));
-        n += popc(brev64(east_sub(brev64(oGen), os)) & targets);
+        n = add_popc(n, brev64(east_sub(brev64(oGen), os)) & targets);
     }
 }
 
@@ -772,7 +788,7 @@ PG_HD u32 count_moves_fused(const Board &b, int ksqIn = -1, int tksqIn = -1, u64
     attacked |= pawn_att_down(tP) | knight_set_att(tN) | PG_TAB(king[tksqIn >= 0 ? tksqIn : ctz(b.kings & theirs)]);
 
     // king
-    n += popc(PG_TAB(king[ksq]) & notMine & ~(attacked | xray));
+    n = add_popc(n, PG_TAB(king[ksq]) & notMine & ~(attacked | xray));
     if (!cm) return n;  // double check: king moves only
 
     // castling (relative squares: king e1, rooks h1/a1), never out of check
@@ -792,7 +808,7 @@ PG_HD u32 count_moves_fused(const Board &b, int ksqIn = -1, int tksqIn = -1, u64
     // and left-capture sets are disjoint and share one popcount; promotions
     // (the eighth rank, the high byte) add three more moves each
     const u64 pl = p1c | cl;
-    n += popc(pl) + popc(cr) + 3 * (popc_byte7(pl) + popc_byte7(cr));
+    n = add_popc(add_popc(n, pl), cr) + 3 * (popc_byte7(pl) + popc_byte7(cr));
 
     // en passant: out of check, or capturing the checking pawn
     const u32 epf = st >> 4;
@@ -819,7 +835,7 @@ PG_HD u32 count_moves_fused(const Board &b, int ksqIn = -1, int tksqIn = -1, u64
     // knights
     const u64 N = b.knights & mine & ~pinned;
     if (PG_KNIGHT_LUT) {
-        for_each_bit(N, [&](int sq) { n += popc(PG_TAB(knight[sq]) & targets); });
+        for_each_bit(N, [&](int sq) { n = add_popc(n, PG_TAB(knight[sq]) & targets); });
     } else {
         n += knight_set_count(N, targets);
     }
