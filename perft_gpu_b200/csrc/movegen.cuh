@@ -835,7 +835,7 @@ PG_HD u32 count_moves_fused(const Board &b, int ksqIn = -1, int tksqIn = -1, u64
     // knights
     const u64 N = b.knights & mine & ~pinned;
     if (PG_KNIGHT_LUT) {
-        for_each_bit(N, [&](int sq) { n = add_popc(n, PG_TAB(knight[sq]) & targets); });
+        for_each_bit(N, [&](int sq) { n += popc(PG_TAB(knight[sq]) & targets); });  // a loop: keep the short IADD3 latency
     } else {
         n += knight_set_count(N, targets);
     }
